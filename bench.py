@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Jacobian builds/s of the Newton-shooting solver on B200.
+
+Workload (the metric's configuration): D = 4, Ntau = 1024, NLeft = NRight =
+4000 (8000 spatial points), Gauss-Legendre IRK2, PrecisionIRK 1e-15 -- the
+reference's data/simulation_4D_1024.json setup -- with seeded free data.  One
+step = one finite-difference Jacobian build: 768 columns, each a two-sided
+shoot (1536 IRK sweeps of 4000 steps), as NewtonSolver::assembleJacobian
+(NewtonSolver.cpp:615-702) computes it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Multi-GPU: one process per GPU (torchrun); every rank builds the Jacobian of
+its own seeded solve (independent work, no data-path collective) and `value`
+is all ranks' builds divided by the slowest rank's device time (weak scaling).
+--impl reference times the reference's own CPU implementation (oracle/_ref,
+OpenMP over Jacobian columns, all host threads) on a bounded column sample.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+PKG = REPO / "parallel-critical-collapse_b200"
+sys.path.insert(0, str(PKG))
+
+METRIC = "Jacobian builds/s at Nτ=1024×8000 pts, mixed vs FP64; p50/p99 solve latency"
+FIXTURE = REPO / "tests" / "golden" / "ref_c3_fixture.npz"
+
+
+def f_rhs(n):
+    """Algorithmic FP64 flops of one RHS evaluation: 7 complex FFTs of length
+    Ntau (5 N log2 N each) + 100 flops per point of pointwise work."""
+    return 7 * 5 * n * np.log2(n) + 100 * n
+
+
+def workload(seed, amp):
+    """C3 config and seeded free data.  Free data: the reference's near-solution
+    (data/simulation_4D_1024.json, packed) plus, per field, amp * |c_lead| *
+    N(0,1) * exp(-k/8) on the coefficient of mode k (Delta unchanged)."""
+    d = np.load(FIXTURE)
+    cfg = json.loads(str(d["config"]))
+    in0 = d["in0"].copy()
+    nn = in0.size
+    third = nn // 3
+    rng = np.random.default_rng(seed)
+    islot = 2 * third + 2
+    for f in range(3):
+        blk = in0[f * third:(f + 1) * third]
+        modes = np.arange(third) // 2 * 2 + (1 if f < 2 else 0)  # odd fields: modes 1,3,..; even: 0,2,..
+        lead = np.max(np.abs(blk[:2]))
+        noise = amp * lead * rng.standard_normal(third) * np.exp(-modes / 8.0)
+        if f == 2:
+            noise[islot - 2 * third] = 0.0  # Delta
+            noise[1] = 0.0                  # the shared cosine of mode Ntau/4 (packSpectralFields :710)
+        in0[f * third:(f + 1) * third] = blk + noise
+    return cfg, in0
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def traffic_per_launch():
+    """DRAM bytes per launch of the march kernel from the committed ncu summary."""
+    p = REPO / "profiles" / "march_c3.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_full_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, v):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference(cfg, in0, out0, columns, threads):
+    """Times the reference's own OpenMP Jacobian loop on `columns` columns."""
+    sys.path.insert(0, str(REPO / "tests" / "golden"))
+    from ref_lib import RefLib  # compiled reference (oracle/_ref)
+
+    R = RefLib()
+    t = time.perf_counter()
+    R.jacobian_columns(cfg, in0, out0, 0, columns, threads)
+    return time.perf_counter() - t
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    cfg, in0 = workload(args.seed, args.amp)
+    nn = in0.size
+    sys.path.insert(0, str(REPO / "tests" / "golden"))
+    from ref_lib import RefLib
+
+    if not (REPO / "oracle" / "_ref" / "libpcc_ref.so").exists():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpcc_ref.so was not built"}))
+        return
+    R = RefLib()
+    out0 = R.shoot(cfg, in0)
+    threads = os.cpu_count() or 1
+    cols = min(threads, nn)
+    for _ in range(args.warmup):
+        R.jacobian_columns(cfg, in0, out0, 0, 1, 1)
+    times = [cpu_reference(cfg, in0, out0, cols, threads) for _ in range(args.steps)]
+    per_build = np.array(times) * nn / cols
+    value = 1.0 / float(np.mean(per_build))
+    sample = f"{cols} of {nn} Jacobian columns per step on {threads} threads, extrapolated x{nn / cols:.1f}"
+    line = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": float(np.mean(per_build)) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded free data)",
+            "impl": "reference",
+            "config": {"workload": "C3: D=4, Ntau=1024, 4000+4000 points, 768-column FD Jacobian, IRK2",
+                       "seed": args.seed, "amp": args.amp},
+            "cpu_baseline": {"value": value, "unit": "builds/s", "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_engine(args, world, rank, local):
+    import torch
+
+    import pcc
+
+    torch.cuda.set_device(local)
+    eng = pcc.Engine(local)
+    cfg, in0 = workload(args.seed + rank, args.amp)
+    solve = eng.solve(pcc.SolveDesc.from_config(cfg))
+    nn, n = solve.nn, solve.ntau
+    out0 = solve.shoot(in0)  # base shoot (the Newton step's, outside the build)
+
+    d_in0 = torch.tensor(in0, dtype=torch.float64, device="cuda")
+    d_out0 = torch.tensor(out0, dtype=torch.float64, device="cuda")
+    d_J = torch.empty((nn, nn), dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+    torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        solve.jacobian_device(d_in0.data_ptr(), d_out0.data_ptr(), d_J.data_ptr())
+        solve.sync()
+
+    clocks = Clocks(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dev_ms, sweep_ms, rhs = [], [], 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        solve.jacobian_device(d_in0.data_ptr(), d_out0.data_ptr(), d_J.data_ptr())
+        st = solve.sync()
+        dev_ms.append(st["ms_total"])
+        sweep_ms.append(st["ms_sweep"])
+        rhs += st["rhs_evals"]
+    torch.cuda.synchronize()
+    barrier(world)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    total_ms = max_over_ranks(world, float(np.sum(dev_ms)))
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms * 1e-3)
+
+    # end to end: the host C-ABI call with pinned host buffers, copies included
+    h_in0 = torch.tensor(in0, dtype=torch.float64).pin_memory()
+    h_out0 = torch.tensor(out0, dtype=torch.float64).pin_memory()
+    h_J = torch.empty((nn, nn), dtype=torch.float64).pin_memory()
+    lib = pcc.load()
+    D = pcc._D
+    import ctypes
+
+    def ptr(t):
+        return ctypes.cast(ctypes.c_void_p(t.data_ptr()), D)
+
+    st_e = pcc.Stats()
+    barrier(world)
+    t1 = time.perf_counter()
+    for _ in range(args.steps):
+        r = lib.pcc_jacobian(solve.h, ptr(h_in0), ptr(h_out0), ptr(h_J), ctypes.byref(st_e))
+        if r != 0:
+            raise pcc.PccError(r, lib.pcc_last_error(eng.ctx).decode())
+    barrier(world)
+    e2e_s = max_over_ranks(world, time.perf_counter() - t1)
+    e2e = {"value": world * args.steps / e2e_s, "unit": "builds/s", "h2d_bytes_per_step": 2 * nn * 8,
+           "d2h_bytes_per_step": nn * nn * 8}
+    if not np.all(np.isfinite(h_J.numpy())):
+        raise RuntimeError("non-finite Jacobian")
+
+    peak = eng.fp64_peak_tflops()
+    flops_per_launch = (rhs / args.steps) * f_rhs(n)
+    achieved = flops_per_launch / (np.mean(sweep_ms) * 1e-3) / 1e12
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": traffic_per_launch(), "kernel": "march_kernel<1024,2>",
+                "peak_source": "in-run FP64 FMA probe (MEASURED_PEAKS.json has no FP64 figure)",
+                "flops_per_launch": flops_per_launch, "rhs_evals_per_launch": rhs / args.steps,
+                "flop_convention": "7*5*N*log2(N) + 100*N per RHS evaluation (reference algorithm)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        ref_so = REPO / "oracle" / "_ref" / "libpcc_ref.so"
+        threads = os.cpu_count() or 1
+        cols = min(threads, nn)
+        if ref_so.exists():
+            t = cpu_reference(cfg, in0, out0, cols, threads)
+            cpu = {"value": (cols / nn) / t, "unit": "builds/s", "cores": threads, "kind": "reference",
+                   "sample": f"{cols} of {nn} Jacobian columns on {threads} threads ({t:.1f} s), extrapolated"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded free data)",
+                "config": {"workload": "C3: D=4, Ntau=1024, 4000+4000 points, 768-column FD Jacobian, IRK2",
+                           "ntau": n, "points": cfg["NLeft"] + cfg["NRight"], "columns": nn, "seed": args.seed,
+                           "amp": args.amp, "l2": "flushed (256 MB write) before every timed build",
+                           "parallelism": f"{world} independent solves, one per GPU",
+                           "sweep_ctas": st_e.sweep_ctas, "wall_s": wall},
+                "clocks": clk, "e2e": e2e, "gpu_launches": 4 * args.steps, "roofline": roofline,
+                "cpu_baseline": cpu}
+        print(json.dumps(line))
+    solve.close()
+    eng.close()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--seed", type=int, default=1024)
+    ap.add_argument("--amp", type=float, default=0.1)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_engine(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

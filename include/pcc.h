@@ -1,0 +1,166 @@
+/*
+ * pcc.h -- C ABI of the B200 Newton-shooting engine for discretely
+ * self-similar critical collapse (the hot path of
+ * tobjec/parallel-critical-collapse: the finite-difference Jacobian whose
+ * columns are independent two-sided IRK shoots, and the dense Newton solve).
+ *
+ * Plain C: pointers and sizes only.  Host pointers are caller-owned; device
+ * buffers are owned by a pcc_solve.  Every call is ordered on the context's
+ * single CUDA stream and the host-pointer variants synchronise before they
+ * return.  No call exits the process: failures come back as pcc_status, with
+ * the failing column, side and grid index in pcc_stats.
+ *
+ * Conventions shared with the reference (all arrays FP64):
+ *   Ntau        collocation points per echoing period (power of two, 128..2048)
+ *   Nnewton     3*Ntau/4 Newton unknowns; in0[2*Nnewton/3+2] holds Delta
+ *   state Y     Ntau/2 complex Fourier modes stored as Ntau interleaved reals,
+ *               Re Y[2] = Delta (ODEStepper.cpp:92-136)
+ *   J           Nnewton x Nnewton, row-major, J[row*Nnewton + col]
+ *               = (F(in0 + eps e_col)[row] - out0[row]) / eps
+ */
+#ifndef PCC_H
+#define PCC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PCC_OK = 0,
+    PCC_ERR_INVALID_ARG = 1,
+    PCC_ERR_CUDA = 2,
+    PCC_ERR_OOM = 3,
+    PCC_ERR_IRK_NO_CONVERGENCE = 4, /* ShootingSolver.cpp:69-82,112-125 exit */
+    PCC_ERR_DELTA_MISMATCH = 5,     /* ShootingSolver.cpp:167-178 exit */
+    PCC_ERR_NAN = 6,
+    PCC_ERR_LU_SINGULAR = 7,        /* NewtonSolver.cpp:751-755 exit */
+    PCC_ERR_IR_STALL = 8,
+    PCC_ERR_UNSUPPORTED = 9,
+    PCC_ERR_NEWTON_NO_CONVERGENCE = 10, /* NewtonSolver.cpp:368-372 exit */
+    PCC_ERR_BUSY = 11
+} pcc_status;
+
+typedef enum {
+    PCC_PREC_FP64 = 0,  /* LU with partial pivoting in FP64 (LAPACKE_dgesv semantics) */
+    PCC_PREC_MIXED = 1  /* FP32 LU + FP64 iterative refinement */
+} pcc_precision;
+
+typedef struct pcc_ctx pcc_ctx;
+typedef struct pcc_solve pcc_solve;
+
+typedef struct {
+    int reserved; /* must be 0 */
+} pcc_ctx_opts;
+
+/* The numeric fields of the reference's SimulationConfig
+ * (include/SimulationConfig.hpp:37-50) that the shooting path reads. */
+typedef struct {
+    int ntau;            /* Ntau */
+    double dim;          /* Dim (D) */
+    double xl, xm, xr;   /* XLeft, XMid, XRight */
+    double eps_newton;   /* EpsNewton */
+    int nl, nr;          /* NLeft, NRight */
+    double prec_irk;     /* PrecisionIRK */
+    int scheme;          /* SchemeIRK: 1, 2 or 3 Gauss-Legendre stages */
+    int max_irk;         /* MaxIterIRK */
+    double prec_newton;  /* PrecisionNewton */
+    double slow_error;   /* SlowError (Newton damping) */
+    int max_newton;      /* MaxIterNewton */
+} pcc_solve_desc;
+
+typedef struct {
+    long long rhs_evals;      /* RHS evaluations performed on the device */
+    long long irk_iterations; /* fixed-point iterations summed over all steps */
+    long long irk_steps;      /* grid steps marched */
+    long long shoots;         /* two-sided shoots (Jacobian columns + base) */
+    double ms_prologue;       /* boundary data kernel (device time) */
+    double ms_sweep;          /* IRK march kernel (device time) */
+    double ms_epilogue;       /* mismatch/pack/difference kernels (device time) */
+    double ms_total;          /* whole call incl. copies (device time) */
+    int fail_column;          /* first failing column (-1: none; Nnewton: base) */
+    int fail_side;            /* 0 left sweep, 1 right sweep */
+    int fail_grid_index;      /* grid index the failing IRK step started from */
+    int sweep_ctas;           /* persistent CTAs of the march kernel */
+} pcc_stats;
+
+typedef struct {
+    double rel_err_vs_fp64; /* ||dx - dx_fp64|| / ||dx_fp64|| when checked, else -1 */
+    double residual_norm;   /* ||b - A dx||_inf / (||A||_inf ||dx||_inf) after refinement */
+    int refinement_steps;
+    int fell_back_to_fp64;
+    double ms;
+} pcc_refine_report;
+
+/* Context: one CUDA device, one stream.  NewtonSolver.hpp:150 (ctor) owner. */
+pcc_status pcc_ctx_create(int device, const pcc_ctx_opts* opts, pcc_ctx** out);
+pcc_status pcc_ctx_destroy(pcc_ctx* ctx);
+const char* pcc_status_string(pcc_status s);
+const char* pcc_last_error(pcc_ctx* ctx);
+
+/* Solve: device buffers, grid and tables for one SimulationConfig
+ * (NewtonSolver.cpp:18-52 ctor + generateGrid :477-519). */
+pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve** out);
+pcc_status pcc_solve_destroy(pcc_solve* s);
+pcc_status pcc_solve_grid(pcc_solve* s, double* grid_out /* nl+nr+1 */);
+
+/* NewtonSolver::shoot (NewtonSolver.cpp:403-423): in0 -> out0, host arrays. */
+pcc_status pcc_shoot(pcc_solve* s, const double* in0, double* out0, pcc_stats* stats);
+
+/* NewtonSolver::assembleJacobian (NewtonSolver.cpp:615-702): all Nnewton
+ * columns in one persistent launch; host arrays, J row-major. */
+pcc_status pcc_jacobian(pcc_solve* s, const double* in0, const double* out0, double* J, pcc_stats* stats);
+
+/* The same on device pointers (inputs already resident in HBM); asynchronous
+ * on the context stream, stats filled after pcc_solve_sync. */
+pcc_status pcc_jacobian_device(pcc_solve* s, const double* d_in0, const double* d_out0, double* d_J);
+pcc_status pcc_solve_sync(pcc_solve* s, pcc_stats* stats);
+
+/* Columns [c0, c1) only (c1 may be Nnewton+1 to include the base shoot, whose
+ * output then lands in out_base).  cols is column-major (c1-c0) x Nnewton. */
+pcc_status pcc_jacobian_columns(pcc_solve* s, const double* in0, const double* out0, int c0, int c1,
+                                double* cols, pcc_stats* stats);
+
+/* NewtonSolver::solveLinearSystem (NewtonSolver.cpp:739-757): A x = rhs,
+ * A row-major n x n.  FP64 LU, or FP32 LU refined to FP64. */
+pcc_status pcc_lu_solve(pcc_ctx* ctx, int n, const double* A, const double* rhs, double* x, pcc_precision prec,
+                        pcc_refine_report* report);
+
+/* One iteration of NewtonSolver::run's loop (NewtonSolver.cpp:279-366):
+ * shoot, Jacobian, solve, damped update of in0 (in place).  err_out gets the
+ * RMS mismatch before the update. */
+pcc_status pcc_newton_step(pcc_solve* s, double* in0, double* err_out, pcc_precision prec, pcc_stats* stats,
+                           pcc_refine_report* report);
+
+/* ---- lower-level entry points (the reference's inner class methods) ---- */
+
+/* ODEStepper::computeDerivatives (ODEStepper.cpp:92-136) for `count` states:
+ * y and dy are count x Ntau, x has count entries. */
+pcc_status pcc_rhs_eval(pcc_ctx* ctx, int ntau, double dim, int count, const double* y, const double* x,
+                        double* dy);
+
+/* ODEStepper::stepIRK (ODEStepper.cpp:163-292) for `count` independent states
+ * (x_in, x_out per state).  its_out (count ints) may be NULL. */
+pcc_status pcc_irk_step(pcc_ctx* ctx, int ntau, double dim, int scheme, double precision, int max_its, int count,
+                        const double* y_in, const double* x_in, const double* x_out, double* y_out, int* its_out);
+
+/* InitialConditionGenerator::computeLeftExpansion / computeRightExpansion after
+ * unpackSpectralFields, as NewtonSolver::shoot performs them (:408-415):
+ * y_left and y_right are Ntau reals each. */
+pcc_status pcc_boundary_data(pcc_solve* s, const double* in0, double* y_left, double* y_right);
+
+/* ShootingSolver::integrateToMatchPoint (ShootingSolver.cpp:53-145) for
+ * `count` states on the solve's grid; side 0 marches x_L -> x_M, side 1
+ * x_R -> x_M. */
+pcc_status pcc_sweep(pcc_solve* s, int count, const int* sides, const double* y_init, double* y_final,
+                     pcc_stats* stats);
+
+/* Measured FP64 FMA throughput of this device in TFLOP/s (a short probe). */
+pcc_status pcc_fp64_peak(pcc_ctx* ctx, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PCC_H */

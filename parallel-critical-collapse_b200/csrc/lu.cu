@@ -1,0 +1,375 @@
+// lu.cu -- dense Newton solve (NewtonSolver::solveLinearSystem,
+// NewtonSolver.cpp:739-757, which calls LAPACKE_dgesv on the row-major J).
+//
+// Blocked right-looking LU with partial pivoting on a row-major matrix, the
+// algorithm of LAPACK dgetrf/dgetrs: per panel of NB columns a single-CTA
+// panel factorisation (pivot = first entry of maximal modulus, as idamax; the
+// whole row is swapped; multipliers scaled by the reciprocal pivot as dgetf2
+// does), a triangular solve for the U12 block row, and a tiled rank-NB update
+// of the trailing matrix spread over the GPU.  Templated on the working type:
+// FP64 for the reference-equivalent solve, FP32 for the mixed-precision solve,
+// which is refined to FP64 accuracy with FP64 residuals as LAPACK dsgesv does
+// (stop when ||r||_inf <= sqrt(n) eps ||A||_inf ||x||_inf, at most 30 sweeps,
+// else fall back to the FP64 factorisation).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pcc_internal.h"
+
+namespace pcc {
+
+namespace {
+
+constexpr int kNB = 32;
+
+template <typename T>
+__global__ void __launch_bounds__(256) panel_kernel(T* A, int n, int k0, int nb, int* ipiv, int* info)
+{
+    __shared__ T smax[256];
+    __shared__ int sidx[256];
+    __shared__ T piv_s;
+    __shared__ int p_s;
+    const int tid = threadIdx.x;
+    const int kend = min(k0 + nb, n);
+    for (int j = k0; j < kend; ++j) {
+        // pivot: first row of maximal |A[i][j]|, i >= j
+        T best = -1;
+        int bi = j;
+        for (int i = j + tid; i < n; i += blockDim.x) {
+            const T v = fabs(A[(size_t)i * n + j]);
+            if (v > best) {
+                best = v;
+                bi = i;
+            }
+        }
+        smax[tid] = best;
+        sidx[tid] = bi;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (tid < o) {
+                const T a = smax[tid], b = smax[tid + o];
+                const int ia = sidx[tid], ib = sidx[tid + o];
+                if (b > a || (b == a && ib < ia)) {
+                    smax[tid] = b;
+                    sidx[tid] = ib;
+                }
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            p_s = sidx[0];
+            ipiv[j] = sidx[0];
+            if (smax[0] == 0 && info[0] == 0) info[0] = j + 1;
+        }
+        __syncthreads();
+        const int p = p_s;
+        if (p != j) {
+            for (int c = tid; c < n; c += blockDim.x) {
+                const T t = A[(size_t)j * n + c];
+                A[(size_t)j * n + c] = A[(size_t)p * n + c];
+                A[(size_t)p * n + c] = t;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) piv_s = A[(size_t)j * n + j];
+        __syncthreads();
+        const T piv = piv_s;
+        if (piv != 0) {
+            const T r = T(1) / piv;
+            for (int i = j + 1 + tid; i < n; i += blockDim.x) A[(size_t)i * n + j] *= r;
+        }
+        __syncthreads();
+        // rank-1 update inside the panel
+        const int w = kend - j - 1;
+        if (w > 0) {
+            for (int e = tid; e < (n - j - 1) * w; e += blockDim.x) {
+                const int i = j + 1 + e / w, c = j + 1 + e % w;
+                A[(size_t)i * n + c] -= A[(size_t)i * n + j] * A[(size_t)j * n + c];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// U12 = L11^{-1} A12 for the block row [k0, k0+nb), columns >= k0+nb
+template <typename T>
+__global__ void trsm_kernel(T* A, int n, int k0, int nb)
+{
+    const int c = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    for (int r = 1; r < nb; ++r) {
+        T s = A[(size_t)(k0 + r) * n + c];
+        for (int l = 0; l < r; ++l) s -= A[(size_t)(k0 + r) * n + k0 + l] * A[(size_t)(k0 + l) * n + c];
+        A[(size_t)(k0 + r) * n + c] = s;
+    }
+}
+
+// A22 -= L21 U12, 64x64 tiles, 256 threads, 4x4 outputs per thread
+template <typename T>
+__global__ void __launch_bounds__(256) update_kernel(T* A, int n, int k0, int nb)
+{
+    __shared__ T Ls[64][kNB + 1];
+    __shared__ T Us[kNB][64 + 1];
+    const int k1 = k0 + nb;
+    const int r0 = k1 + blockIdx.y * 64, c0 = k1 + blockIdx.x * 64;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < 64 * nb; e += 256) {
+        const int i = e / nb, l = e % nb;
+        Ls[i][l] = (r0 + i < n) ? A[(size_t)(r0 + i) * n + k0 + l] : T(0);
+    }
+    for (int e = tid; e < nb * 64; e += 256) {
+        const int l = e / 64, c = e % 64;
+        Us[l][c] = (c0 + c < n) ? A[(size_t)(k0 + l) * n + c0 + c] : T(0);
+    }
+    __syncthreads();
+    const int ty = tid / 16, tx = tid % 16;
+    T acc[4][4] = {};
+    for (int l = 0; l < nb; ++l) {
+        T a[4], b[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a[u] = Ls[ty + 16 * u][l];
+            b[u] = Us[l][tx + 16 * u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] += a[u] * b[v];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int r = r0 + ty + 16 * u;
+        if (r >= n) continue;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int c = c0 + tx + 16 * v;
+            if (c < n) A[(size_t)r * n + c] -= acc[u][v];
+        }
+    }
+}
+
+template <typename T>
+cudaError_t lu_factor(T* A, int n, int* ipiv, int* info, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    for (int k0 = 0; k0 < n; k0 += kNB) {
+        const int nb = min(kNB, n - k0);
+        panel_kernel<T><<<1, 256, 0, st>>>(A, n, k0, nb, ipiv, info);
+        const int rest = n - k0 - nb;
+        if (rest > 0) {
+            trsm_kernel<T><<<(rest + 127) / 128, 128, 0, st>>>(A, n, k0, nb);
+            dim3 g((rest + 63) / 64, (rest + 63) / 64);
+            update_kernel<T><<<g, 256, 0, st>>>(A, n, k0, nb);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// x = A^{-1} b from the factors (dgetrs): row swaps, unit-lower forward and
+// upper backward substitution.  One CTA; TB is the type of the vectors.
+template <typename T, typename TB>
+__global__ void __launch_bounds__(1024) lu_apply_kernel(const T* A, int n, const int* ipiv, const TB* b, TB* x)
+{
+    const int tid = threadIdx.x;
+    if (tid == 0)
+        for (int i = 0; i < n; ++i) x[i] = b[i];
+    __syncthreads();
+    if (tid == 0)
+        for (int i = 0; i < n; ++i) {
+            const int p = ipiv[i];
+            if (p != i) {
+                const TB t = x[i];
+                x[i] = x[p];
+                x[p] = t;
+            }
+        }
+    __syncthreads();
+    for (int j = 0; j < n; ++j) {
+        const TB yj = x[j];
+        for (int i = j + 1 + tid; i < n; i += blockDim.x) x[i] -= (TB)A[(size_t)i * n + j] * yj;
+        __syncthreads();
+    }
+    for (int j = n - 1; j >= 0; --j) {
+        if (tid == 0) x[j] = x[j] / (TB)A[(size_t)j * n + j];
+        __syncthreads();
+        const TB yj = x[j];
+        for (int i = tid; i < j; i += blockDim.x) x[i] -= (TB)A[(size_t)i * n + j] * yj;
+        __syncthreads();
+    }
+}
+
+__global__ void to_float_kernel(const double* a, float* b, size_t cnt)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+// r = b - A x (FP64), one warp per row; out[0] = ||r||_inf, out[1] = ||x||_inf
+__global__ void residual_kernel(const double* A, const double* b, const double* x, double* r, int n,
+                                unsigned long long* norms)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s = fma(A[(size_t)warp * n + j], x[j], s);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        const double ri = b[warp] - s;
+        r[warp] = ri;
+        atomicMax(&norms[0], __double_as_longlong(fabs(ri)));
+        atomicMax(&norms[1], __double_as_longlong(fabs(x[warp])));
+    }
+}
+
+// ||A||_inf
+__global__ void rownorm_kernel(const double* A, int n, unsigned long long* out)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s += fabs(A[(size_t)warp * n + j]);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) atomicMax(out, __double_as_longlong(s));
+}
+
+__global__ void axpy_kernel(double* x, const double* d, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += d[i];
+}
+
+__global__ void fma_probe_kernel(double* out, int iters, double seed)
+{
+    double a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+           a7 = a0 + 7;
+    const double m = 0.999999, c = 1e-7;
+    for (int i = 0; i < iters; ++i) {
+        a0 = fma(a0, m, c);
+        a1 = fma(a1, m, c);
+        a2 = fma(a2, m, c);
+        a3 = fma(a3, m, c);
+        a4 = fma(a4, m, c);
+        a5 = fma(a5, m, c);
+        a6 = fma(a6, m, c);
+        a7 = fma(a7, m, c);
+    }
+    if (a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7 == 12345.678) out[0] = 1.0;
+}
+
+}  // namespace
+
+size_t lu_mixed_work_bytes(int n)
+{
+    // float copy of A, r and d vectors (double), norms
+    return (size_t)n * n * sizeof(float) + 4 * (size_t)n * sizeof(double) + 64;
+}
+
+cudaError_t lu_solve_fp64(const double* dA, const double* db, double* dx, int n, double* work, int* ipiv, int* info,
+                          cudaStream_t st)
+{
+    (void)work;
+    double* A = const_cast<double*>(dA);  // factorised in place (the caller's working copy)
+    cudaError_t e = lu_factor<double>(A, n, ipiv, info, st);
+    if (e != cudaSuccess) return e;
+    lu_apply_kernel<double, double><<<1, 1024, 0, st>>>(A, n, ipiv, db, dx);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int zero = 0;
+    return cudaMemcpyAsync(info + 1, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+}
+
+cudaError_t lu_solve_mixed(const double* dA, const double* db, double* dx, int n, void* work, size_t work_bytes,
+                           int* ipiv, int* info, int max_refine, double tol, int* steps_out, double* resid_out,
+                           cudaStream_t st)
+{
+    (void)work_bytes;
+    (void)tol;
+    float* A32 = static_cast<float*>(work);
+    double* r = reinterpret_cast<double*>(A32 + (size_t)n * n);
+    double* d = r + n;
+    unsigned long long* norms = reinterpret_cast<unsigned long long*>(d + 2 * n);
+    cudaError_t e;
+    const size_t nn = (size_t)n * n;
+    to_float_kernel<<<1024, 256, 0, st>>>(dA, A32, nn);
+    if ((e = lu_factor<float>(A32, n, ipiv, info, st)) != cudaSuccess) return e;
+    // ||A||_inf
+    if ((e = cudaMemsetAsync(norms, 0, 3 * sizeof(unsigned long long), st)) != cudaSuccess) return e;
+    rownorm_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(dA, n, norms + 2);
+    // x0 = LU32 \ b (computed in FP64 on the FP32 factors)
+    lu_apply_kernel<float, double><<<1, 1024, 0, st>>>(A32, n, ipiv, db, dx);
+    unsigned long long h[3];
+    int hinfo = 0;
+    if ((e = cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    const double eps = 1.1102230246251565e-16;  // dlamch('Epsilon')
+    int steps = 0, fallback = (hinfo != 0) ? 1 : 0;
+    double resid = -1.0;
+    bool ok = false;
+    for (; !fallback && steps <= max_refine; ++steps) {
+        if ((e = cudaMemsetAsync(norms, 0, 2 * sizeof(unsigned long long), st)) != cudaSuccess) return e;
+        residual_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(dA, db, dx, r, n, norms);
+        if ((e = cudaMemcpyAsync(h, norms, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return e;
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+        double rn, xn, an;
+        std::memcpy(&rn, &h[0], 8);
+        std::memcpy(&xn, &h[1], 8);
+        std::memcpy(&an, &h[2], 8);
+        resid = (an > 0 && xn > 0) ? rn / (an * xn) : rn;
+        if (!std::isfinite(resid)) break;
+        if (rn <= std::sqrt((double)n) * eps * an * xn) {
+            ok = true;
+            break;
+        }
+        if (steps == max_refine) break;
+        lu_apply_kernel<float, double><<<1, 1024, 0, st>>>(A32, n, ipiv, r, d);
+        axpy_kernel<<<(n + 255) / 256, 256, 0, st>>>(dx, d, n);
+    }
+    if (steps_out) *steps_out = steps;
+    if (resid_out) *resid_out = resid;
+    if (!ok) {
+        // LAPACK dsgesv falls back to dgetrf/dgetrs in double precision
+        double* A = const_cast<double*>(dA);
+        if ((e = lu_factor<double>(A, n, ipiv, info, st)) != cudaSuccess) return e;
+        lu_apply_kernel<double, double><<<1, 1024, 0, st>>>(A, n, ipiv, db, dx);
+        fallback = 1;
+    } else {
+        int zero = 0;
+        if ((e = cudaMemcpyAsync(info, &zero, sizeof(int), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    }
+    if ((e = cudaMemcpyAsync(info + 1, &fallback, sizeof(int), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    return cudaStreamSynchronize(st);
+}
+
+cudaError_t fp64_peak_probe(double* tflops, cudaStream_t st)
+{
+    int dev = 0, sms = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    double* out = nullptr;
+    if ((e = cudaMalloc(&out, sizeof(double))) != cudaSuccess) return e;
+    const int blocks = sms * 8, threads = 256, iters = 1 << 15;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    fma_probe_kernel<<<blocks, threads, 0, st>>>(out, 1024, 1.0);  // warm-up
+    cudaEventRecord(a, st);
+    fma_probe_kernel<<<blocks, threads, 0, st>>>(out, iters, 1.0);
+    cudaEventRecord(b, st);
+    e = cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    if (e != cudaSuccess) return e;
+    const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return cudaSuccess;
+}
+
+}  // namespace pcc

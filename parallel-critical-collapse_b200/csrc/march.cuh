@@ -1,0 +1,658 @@
+// march.cuh -- the hot path: persistent FP64 Gauss-Legendre IRK march of the
+// shooting sweeps (ShootingSolver::integrateToMatchPoint, ShootingSolver.cpp:
+// 53-145; ODEStepper::stepIRK, ODEStepper.cpp:163-292; ODEStepper::
+// computeDerivatives, ODEStepper.cpp:92-136; InitialConditionGenerator::
+// StateVectorToFields/FieldsToStateVector, InitialConditionGenerator.cpp:
+// 766-884; SpectralTransformer::solveInhom, SpectralTransformer.cpp:264-292).
+//
+// Work unit ("sweep"): one (Jacobian column, side) pair, marched over all grid
+// steps of that side by S stage groups of TG = Ntau/16 threads (one group per
+// IRK stage).  Persistent sweep slots pull sweeps from an atomic counter.
+//
+// Half-length spectral formulation.  The reference evaluates each RHS with
+// seven complex FFTs of length N = Ntau on the band-limited state Y (N/2
+// modes, |m| <= N/4).  U and V are anti-periodic over half an echoing period
+// (odd Fourier modes only) and F, IA2 are periodic over half a period (even
+// modes only), so with M = N/2 and w = exp(-2 pi i/N):
+//   U_j + i V_j = w^j   * IDFT_M(c_odd)_j        (c_odd[k'] = c[2k'+1])
+//   F_j         = Im IDFT_M(c_even)_j            (c_even[k'] = c[2k'])
+//   dU, dV      = the same with c -> -i m k0 c
+//   solveInhom  : four length-M transforms of real half-period data
+//   Y'[odd 2k'+1] = DFT_M((dUdx + i dVdx) w^-j)/M, Y'[even 2k'] = DFT_M(i dFdx)/M
+// for j < M, which equals the reference's split
+//   U = (Re Z_j - Re Z_{j+M})/2, F = (Im Z_j + Im Z_{j+M})/2, ...
+// (InitialConditionGenerator.cpp:849-874) exactly in real arithmetic.  The
+// quirks of the reference are kept: doubleModes stores the full Y[N/4] at
+// index 3N/4 and half of it at N/4 (SpectralTransformer.cpp:238-245), the
+// phase fix Re c[2] = -Re c[N-2] (InitialConditionGenerator.cpp:800), and the
+// frozen Delta slot Re dY[2] = 0 (ODEStepper.cpp:128).
+//
+// Data layout per thread t of a stage group: DFT position p_q = t + TG q,
+// q = 0..7, serves both as physical point j and as spectral index k'.  The
+// state modes a thread owns are exactly those its positions q in {0,1,6,7}
+// produce ("slots": sigma = 2*ri + parity, ri -> q in {0,1,6,7}), so every
+// state array is slot-indexed [sigma][t] and the IRK update touches only the
+// thread's own entries.  Shared memory per sweep: y, the stage values yk, and
+// two exchange buffers per stage; the stage RHS f is written into the
+// exchange buffer that the next transform writes first, which is idle from
+// the end of one RHS evaluation to the start of the next.
+#pragma once
+#include "pcc_device.cuh"
+
+namespace pcc {
+
+struct MarchParams {
+    int n_items;
+    int mode;                       // 0 march, 1 single RHS evaluation, 2 single IRK step
+    const double* __restrict__ yinit;  // [item][N], interleaved modes
+    double* __restrict__ yfinal;       // [item][N]
+    const int* __restrict__ item_side; // optional, else side = item & 1
+    const double* __restrict__ grid;   // nl + nr + 1
+    int nl, nr;
+    double dim;
+    double dim_m2_cubed;  // std::pow(Dim - 2.0, 3) as computed by the host
+    double prec;
+    int max_its;
+    int stages;
+    double a[3][3], b[3], c[3];
+    const double2* __restrict__ twN;   // exp(+2 pi i k/N), k < N
+    const double* __restrict__ x_in;   // [item] (modes 1 and 2)
+    const double* __restrict__ x_out;  // [item] (mode 2)
+    int* work_counter;
+    int* status;       // [item]: 0 ok, 1 IRK no convergence
+    int* fail_index;   // [item]: grid index the failing step started from
+    int* its_out;      // [item] (mode 2), may be null
+    unsigned long long* counters;  // [0] RHS evaluations [1] IRK iterations [2] steps
+};
+
+template <int N, int S>
+struct MarchShape {
+    static constexpr int M = N / 2;
+    static constexpr int Q = N / 4;
+    static constexpr int TG = M / 8;        // threads per stage group
+    static constexpr int ST = S * TG;       // working threads per sweep
+    // padded sweep width: power of two below a warp, else a multiple of 32
+    static constexpr int STP = ST <= 8 ? 8 : ST <= 16 ? 16 : ST <= 32 ? 32 : ((ST + 31) / 32) * 32;
+    static constexpr int SPC = STP >= 128 ? 1 : 128 / STP;  // sweeps per CTA
+    static constexpr int NT = SPC * STP;                      // threads per CTA
+    static constexpr int NW = STP >= 32 ? STP / 32 : 1;       // warps per sweep
+    static constexpr int MP = M;                              // exchange length (swizzled)
+    static constexpr int EX = S * 2 * MP;                     // exchange double2s
+    static constexpr int YS = 8 * TG;                         // slot-indexed y
+    static constexpr int YK = S * 8 * TG;                     // slot-indexed stage values
+    static constexpr int UV = S * M;                          // U and V per stage (doubles -> M double2)
+    static constexpr int MISC = (S + NW + 1) / 2 + 2;          // lam, red, item, zero (in double2)
+    static constexpr int PER_SWEEP = EX + YS + YK + UV + MISC; // double2 per sweep
+    static constexpr size_t SMEM = (size_t)SPC * PER_SWEEP * sizeof(double2);
+    static constexpr int NP = M == 64 ? 2 : (M <= 512 ? 3 : 4);
+    static constexpr int R_LAST = M == 64 ? 8 : M == 128 ? 2 : M == 256 ? 4 : M == 512 ? 8 : 2;
+};
+
+// ---------------------------------------------------------------- DFT kernels
+template <int SG>
+__device__ __forceinline__ void dft2(double2& a0, double2& a1)
+{
+    const double2 t = a0;
+    a0 = cadd(t, a1);
+    a1 = csub(t, a1);
+}
+
+template <int SG>
+__device__ __forceinline__ void dft4(double2& b0, double2& b1, double2& b2, double2& b3)
+{
+    const double2 t0 = cadd(b0, b2), t1 = csub(b0, b2);
+    const double2 t2 = cadd(b1, b3), t3 = cmul_si<SG>(csub(b1, b3));
+    b0 = cadd(t0, t2);
+    b2 = csub(t0, t2);
+    b1 = cadd(t1, t3);
+    b3 = csub(t1, t3);
+}
+
+// X_k = sum_r a_r exp(SG 2 pi i r k / 8): radix-2 decimation in frequency on
+// the array in place, outputs in natural order.
+template <int SG>
+__device__ __forceinline__ void dft8(double2 (&a)[8])
+{
+    constexpr double c = 0.70710678118654752440;
+    // stage 1: butterflies (r, r+4), twiddle W8^r on the difference
+    dft2<SG>(a[0], a[4]);
+    dft2<SG>(a[1], a[5]);
+    dft2<SG>(a[2], a[6]);
+    dft2<SG>(a[3], a[7]);
+    a[5] = make_double2(c * (a[5].x - SG * a[5].y), c * (a[5].y + SG * a[5].x));
+    a[6] = cmul_si<SG>(a[6]);
+    a[7] = make_double2(c * (-a[7].x - SG * a[7].y), c * (-a[7].y + SG * a[7].x));
+    // stage 2: butterflies (r, r+2) within each half, twiddle W4 on the difference
+    dft2<SG>(a[0], a[2]);
+    dft2<SG>(a[1], a[3]);
+    a[3] = cmul_si<SG>(a[3]);
+    dft2<SG>(a[4], a[6]);
+    dft2<SG>(a[5], a[7]);
+    a[7] = cmul_si<SG>(a[7]);
+    // stage 3
+    dft2<SG>(a[0], a[1]);
+    dft2<SG>(a[2], a[3]);
+    dft2<SG>(a[4], a[5]);
+    dft2<SG>(a[6], a[7]);
+    // bit-reversed -> natural order: swap (1,4), (3,6)
+    double2 t = a[1];
+    a[1] = a[4];
+    a[4] = t;
+    t = a[3];
+    a[3] = a[6];
+    a[6] = t;
+}
+
+// One Stockham pass of radix R over span NS on the standard layout: thread t
+// holds x[t + TG q]; butterfly j = t + TG u takes x[j + r M/R] = v[u + r*8/R].
+template <int M, int TG, int R, int NS, int SG, bool LAST>
+__device__ __forceinline__ void stockham_pass(double2 (&v)[8], double2* __restrict__ out, int t,
+                                              const double2* __restrict__ twN, int zoff)
+{
+    constexpr int B = 8 / R;
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+        const int j = t + TG * u;
+        const int k = j & (NS - 1);
+        double2 a[8];
+#pragma unroll
+        for (int r = 0; r < R; ++r) a[r] = v[u + r * B];
+        if (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                const int idx = r * k * (M / (NS * R));  // exponent of w_M, < M
+                double2 w = __ldg(&twN[2 * idx + zoff]);
+                if (SG < 0) w.y = -w.y;
+                a[r] = cmul(a[r], w);
+            }
+        }
+        if (R == 8) {
+            dft8<SG>(a);
+        } else if (R == 4) {
+            dft4<SG>(a[0], a[1], a[2], a[3]);
+        } else {
+            dft2<SG>(a[0], a[1]);
+        }
+        if (LAST) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[u + r * B] = a[r];
+        } else {
+            const int base = (j / NS) * NS * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) out[swz8(base + r * NS)] = a[r];
+        }
+    }
+}
+
+template <int TG>
+__device__ __forceinline__ void load_std(double2 (&v)[8], const double2* __restrict__ in, int t)
+{
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = in[swz8(t + TG * q)];
+}
+
+// Length-M DFT, X_k = sum_j x_j exp(SG 2 pi i jk/M), unscaled, from and to the
+// standard register layout.  bufs[0..1] ping-pong; `cur` selects the first
+// buffer written and is advanced so that the next transform never writes a
+// buffer that a lagging thread may still be reading.
+template <int M, int TG, int SG>
+__device__ __forceinline__ void dft_m(double2 (&v)[8], double2* __restrict__ b0, double2* __restrict__ b1,
+                                      int& cur, int t, const double2* __restrict__ twN, const SweepSync& sy,
+                                      bool active, const volatile int* zero)
+{
+    constexpr int NP = M == 64 ? 2 : (M <= 512 ? 3 : 4);
+    constexpr int RL = M == 64 ? 8 : M == 128 ? 2 : M == 256 ? 4 : M == 512 ? 8 : 2;
+    double2* w0 = cur ? b1 : b0;
+    double2* w1 = cur ? b0 : b1;
+    if (active) stockham_pass<M, TG, 8, 1, SG, false>(v, w0, t, twN, 0);
+    sy.sync();
+    if (active) load_std<TG>(v, w0, t);
+    // A zero read from shared memory after the barrier, added to every twiddle
+    // index of this transform: the backend cannot prove two transforms use the
+    // same twiddle addresses, so it does not keep all of them live in
+    // registers across the whole RHS evaluation (which costs ~50 registers and
+    // spills).  `zero` is the sweep's constant-zero word.
+    const int zoff = *zero;
+    if constexpr (NP == 2) {
+        if (active) stockham_pass<M, TG, RL, 8, SG, true>(v, w0, t, twN, zoff);
+        cur ^= 1;
+    } else if constexpr (NP == 3) {
+        if (active) stockham_pass<M, TG, 8, 8, SG, false>(v, w1, t, twN, zoff);
+        sy.sync();
+        if (active) load_std<TG>(v, w1, t);
+        if (active) stockham_pass<M, TG, RL, 64, SG, true>(v, w1, t, twN, zoff);
+    } else {
+        if (active) stockham_pass<M, TG, 8, 8, SG, false>(v, w1, t, twN, zoff);
+        sy.sync();
+        if (active) load_std<TG>(v, w1, t);
+        if (active) stockham_pass<M, TG, 8, 64, SG, false>(v, w0, t, twN, zoff);
+        sy.sync();
+        if (active) load_std<TG>(v, w0, t);
+        if (active) stockham_pass<M, TG, RL, 512, SG, true>(v, w0, t, twN, zoff);
+        cur ^= 1;
+    }
+}
+
+// --------------------------------------------------------------- slot maps
+// Slot sigma = 2*ri + parity; ri -> position q in {0, 1, 6, 7}; parity 0 odd
+// modes, 1 even modes.  Returns the state mode index (0..M-1).
+template <int N>
+__device__ __forceinline__ int slot_mode(int sigma, int t)
+{
+    constexpr int M = N / 2, Q = N / 4, TG = M / 8;
+    const int ri = sigma >> 1;
+    const int q = ri < 2 ? ri : ri + 4;
+    const int p = t + TG * q;
+    if ((sigma & 1) == 0) {
+        const int k = 2 * p + 1;
+        return k < Q ? k : k - M;
+    }
+    if (t == 0 && q == 6) return Q;
+    const int k = 2 * p;
+    return k < Q ? k : k - M;
+}
+
+__device__ __forceinline__ int slot_q(int sigma)
+{
+    const int ri = sigma >> 1;
+    return ri < 2 ? ri : ri + 4;
+}
+
+// ------------------------------------------------------------------ the RHS
+// dY/dx of one stage state at x (ODEStepper::computeDerivatives,
+// ODEStepper.cpp:92-136).  yks: this stage's slot-indexed state (shared);
+// b0/b1: this stage's exchange buffers; the result is written slot-indexed
+// into (cur ? b1 : b0), the buffer the next transform would write first.
+template <int N>
+__device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double* __restrict__ uvs, double x,
+                                         double dim, double dm2c, double k0, int t, double2* __restrict__ b0,
+                                         double2* __restrict__ b1, int& cur, double* lam_slot,
+                                         const double2* __restrict__ twN, const SweepSync& sy, bool active,
+                                         const volatile int* zero)
+{
+    constexpr int M = N / 2, TG = M / 8;
+    constexpr double invM = 1.0 / M;
+    double2 v[8];
+    double F[8];
+    double* Us = uvs;      // [q][t], this thread's own entries only
+    double* Vs = uvs + M;
+
+    // --- U + iV from the odd modes (IDFT_M, post-twiddle w^j) ----------------
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = make_double2(0.0, 0.0);
+    if (active) {
+        v[0] = yks[0 * TG + t];
+        v[1] = yks[2 * TG + t];
+        v[6] = yks[4 * TG + t];
+        v[7] = yks[6 * TG + t];
+    }
+    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int j = t + TG * q;
+        const double2 o = cmul(v[q], cconj(__ldg(&twN[j])));
+        if (active) {
+            Us[q * TG + t] = o.x;
+            Vs[q * TG + t] = o.y;
+        }
+    }
+
+    // --- F from the even modes: doubleModes (with its N/4 quirk) + phase fix --
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = make_double2(0.0, 0.0);
+    if (active) {
+        v[0] = yks[1 * TG + t];
+        if (t == 1) v[0].x = -yks[7 * TG + TG - 1].x;  // Re c[2] = -Re c[N-2] = -Re Y[M-2]
+        v[1] = yks[3 * TG + t];
+        const double2 yq = yks[5 * TG + t];
+        if (t == 0) v[2] = make_double2(0.5 * yq.x, 0.5 * yq.y);  // c[N/4] = Y[N/4]/2
+        v[6] = yq;                                                  // c[3N/4] = Y[N/4] (t = 0)
+        v[7] = yks[7 * TG + t];
+    }
+    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) F[q] = v[q].y;
+
+    // --- IA2 constraint coefficients (InitialConditionGenerator.cpp:876-881) --
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const double U = Us[q * TG + t], V = Vs[q * TG + t];
+        const double co = -(((x + F[q]) * U * U + (x - F[q]) * V * V) * dm2c / (8.0 * x) + (dim - 3.0));
+        v[q] = make_double2(co, 0.0);
+    }
+
+    // --- solveInhom (SpectralTransformer.cpp:264-292) on half-period data ----
+    dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = make_double2(v[q].x * invM, v[q].y * invM);
+    if (active && t == 0) *lam_slot = v[0].x;  // lambda = f_hat[0] (real: imag is exactly 0)
+    // lamIntegrate(f_hat, 0): out_k = f_k / (0 - i m k0), DC and Nyquist -> 0
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int p = t + TG * q;
+        const int k = 2 * p;
+        if (p == 0 || k == M) {
+            v[q] = make_double2(0.0, 0.0);
+        } else {
+            const int m = k < M ? k : k - N;
+            v[q] = cdiv(v[q].x, v[q].y, 0.0, 0.0 - m * k0);
+        }
+    }
+    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
+    double Fr[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        Fr[q] = v[q].x;
+        v[q] = make_double2(-(dim - 3.0) * exp(Fr[q]), 0.0);  // h = -g e^F
+    }
+    dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
+    const double lam = *lam_slot;  // written before at least one sweep barrier
+    {
+        const double s = k0 * N / 2.0;
+        const double2 qn = cdiv(lam, 0.0, lam * lam - 0.0 * 0.0 + s * s, lam * 0.0 + 0.0 * lam);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int p = t + TG * q;
+            const int k = 2 * p;
+            const double2 h = make_double2(v[q].x * invM, v[q].y * invM);
+            if (p == 0) {
+                v[q] = lam != 0.0 ? cdiv(h.x, h.y, lam, 0.0) : make_double2(0.0, 0.0);
+            } else if (k == M) {
+                v[q] = cmul(qn, h);
+            } else {
+                const int m = k < M ? k : k - N;
+                const double dr = lam - 0.0, di = 0.0 - m * k0;
+                v[q] = (hypot(dr, di) < 1e-14) ? make_double2(0.0, 0.0) : cdiv(h.x, h.y, dr, di);
+            }
+        }
+    }
+    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
+    double IA2[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) IA2[q] = v[q].x * exp(-Fr[q]);
+
+    // --- dU + i dV from -i m k0 c on the odd modes ---------------------------
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = make_double2(0.0, 0.0);
+    if (active) {
+#pragma unroll
+        for (int ri = 0; ri < 4; ++ri) {
+            const int q = ri < 2 ? ri : ri + 4;
+            const int k = 2 * (t + TG * q) + 1;
+            const int m = k < M ? k : k - N;
+            const double s = m * k0;
+            const double2 a = yks[(2 * ri) * TG + t];
+            v[q] = make_double2(s * a.y, -(s * a.x));
+        }
+    }
+    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
+
+    // --- pointwise Einstein-scalar RHS (ODEStepper.cpp:109-122) ---------------
+    double fx[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int j = t + TG * q;
+        const double2 w = __ldg(&twN[j]);
+        const double2 dO = cmul(v[q], cconj(w));
+        const double dU = dO.x, dV = dO.y;
+        const double U = Us[q * TG + t], V = Vs[q * TG + t];
+        const double ux = (F[q] * ((dim - 2.0) * V - (2.0 * (dim - 3.0) / IA2[q] - (dim - 2.0)) * U) - 2.0 * x * dU) /
+                          (2.0 * x * (F[q] + x));
+        const double vx = (F[q] * ((dim - 2.0) * U - (2.0 * (dim - 3.0) / IA2[q] - (dim - 2.0)) * V) + 2.0 * x * dV) /
+                          (2.0 * x * (F[q] - x));
+        fx[q] = (dim - 3.0) * F[q] * (1.0 - IA2[q]) / (IA2[q] * x);
+        v[q] = cmul(make_double2(ux, vx), w);  // pre-twiddle exp(+2 pi i j/N)
+    }
+
+    // --- FieldsToStateVector: odd modes ---------------------------------------
+    dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
+    const double2 o0 = make_double2(v[0].x * invM, v[0].y * invM);
+    const double2 o1 = make_double2(v[1].x * invM, v[1].y * invM);
+    const double2 o6 = make_double2(v[6].x * invM, v[6].y * invM);
+    const double2 o7 = make_double2(v[7].x * invM, v[7].y * invM);
+    // --- even modes, halveModes fold of N/4 and 3N/4, frozen Delta slot ---------
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = make_double2(0.0, fx[q]);
+    dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
+    if (active) {
+        double2* fslot = cur ? b1 : b0;
+        double2 e0 = make_double2(v[0].x * invM, v[0].y * invM);
+        if (t == 1) e0.x = 0.0;  // dYdx[2] real part (Delta) frozen
+        double2 e6 = make_double2(v[6].x * invM, v[6].y * invM);
+        if (t == 0) e6 = cadd(make_double2(v[2].x * invM, v[2].y * invM), e6);  // in[N/4] + in[3N/4]
+        fslot[0 * TG + t] = o0;
+        fslot[1 * TG + t] = e0;
+        fslot[2 * TG + t] = o1;
+        fslot[3 * TG + t] = make_double2(v[1].x * invM, v[1].y * invM);
+        fslot[4 * TG + t] = o6;
+        fslot[5 * TG + t] = e6;
+        fslot[6 * TG + t] = o7;
+        fslot[7 * TG + t] = make_double2(v[7].x * invM, v[7].y * invM);
+    }
+}
+
+// ------------------------------------------------------------ sweep reduce
+template <int STP, int NW>
+__device__ __forceinline__ double sweep_sum(double x, double* red, int lt, const SweepSync& sy)
+{
+    constexpr int W = STP < 32 ? STP : 32;
+#pragma unroll
+    for (int o = W / 2; o > 0; o >>= 1) x += __shfl_xor_sync(sy.bar_id == 0 ? sy.mask : 0xffffffffu, x, o, 32);
+    if constexpr (NW == 1) {
+        return x;
+    } else {
+        if ((lt & 31) == 0) red[lt >> 5] = x;
+        sy.sync();
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) s += red[w];
+        sy.sync();  // red is reused by the next reduction
+        return s;
+    }
+}
+
+// ------------------------------------------------------------------ kernel
+template <int N, int S, int MINB>
+__global__ void __launch_bounds__(MarchShape<N, S>::NT, MINB) march_kernel(MarchParams P)
+{
+    using K = MarchShape<N, S>;
+    constexpr int TG = K::TG, STP = K::STP;
+    extern __shared__ double2 smem[];
+
+    const int slot_id = threadIdx.x / STP;
+    const int lt = threadIdx.x % STP;
+    const int s_raw = lt / TG;
+    const bool active = s_raw < S;
+    const int s = active ? s_raw : S - 1;
+    const int t = lt % TG;
+
+    SweepSync sy;
+    if constexpr (STP < 32) {
+        sy.bar_id = 0;
+        sy.nthreads = STP;
+        sy.mask = ((1u << STP) - 1u) << ((threadIdx.x & 31) / STP * STP);
+    } else if constexpr (STP == 32) {
+        sy.bar_id = 0;
+        sy.nthreads = 32;
+        sy.mask = 0xffffffffu;
+    } else {
+        sy.bar_id = 1 + slot_id;
+        sy.nthreads = STP;
+        sy.mask = 0xffffffffu;
+    }
+
+    double2* base = smem + (size_t)slot_id * K::PER_SWEEP;
+    double2* ex = base;            // [S][2][MP]; stage RHS lands in one of each pair
+    double2* ys = ex + K::EX;      // [8][TG]
+    double2* yks = ys + K::YS;     // [S][8][TG]
+    double* uv = reinterpret_cast<double*>(yks + K::YK);  // [S][2][M]
+    double* misc = uv + 2 * K::UV;
+    double* lam = misc;            // [S]
+    double* red = misc + S;        // [NW]
+    int* item_slot = reinterpret_cast<int*>(misc + S + K::NW);
+    volatile int* zero_slot = item_slot + 1;
+    if (lt == 0) *zero_slot = 0;
+
+    double2* b0 = ex + (size_t)s * 2 * K::MP;
+    double2* b1 = b0 + K::MP;
+    double2* ykm = yks + (size_t)s * 8 * TG;
+    double* uvm = uv + (size_t)s * 2 * K::M;
+
+    const double dim = P.dim;
+    unsigned long long n_its = 0, n_steps = 0;
+
+    for (;;) {
+        if (lt == 0) *item_slot = atomicAdd(P.work_counter, 1);
+        sy.sync();
+        const int item = *item_slot;
+        sy.sync();
+        if (item >= P.n_items) break;
+
+        const double* yin = P.yinit + (size_t)item * N;
+        const double delta = yin[4];
+        const double k0 = 2.0 * kPi / delta;
+
+        // state -> slots: y (group 0) and every stage value (its own group)
+        if (active) {
+#pragma unroll
+            for (int sg = 0; sg < 8; ++sg) {
+                const int m = slot_mode<N>(sg, t);
+                const double2 v = make_double2(yin[2 * m], yin[2 * m + 1]);
+                ykm[sg * TG + t] = v;
+                if (s == 0) ys[sg * TG + t] = v;
+            }
+        }
+        int cur = 0;
+        sy.sync();
+
+        if (P.mode == 1) {
+            // single RHS evaluation of the state at x_in[item]
+            rhs_eval<N>(ykm, uvm, P.x_in[item], dim, P.dim_m2_cubed, k0, t, b0, b1, cur, &lam[s], P.twN, sy, active, zero_slot);
+            sy.sync();
+            if (active && s == 0) {
+                const double2* fr = cur ? b1 : b0;
+                double* yo = P.yfinal + (size_t)item * N;
+#pragma unroll
+                for (int sg = 0; sg < 8; ++sg) {
+                    const int m = slot_mode<N>(sg, t);
+                    const double2 f = fr[sg * TG + t];
+                    yo[2 * m] = f.x;
+                    yo[2 * m + 1] = f.y;
+                }
+            }
+            sy.sync();
+            continue;
+        }
+
+        const int side = P.item_side ? P.item_side[item] : (item & 1);
+        const int nsteps = P.mode == 2 ? 1 : (side == 0 ? P.nl : P.nr);
+        int status = 0, fail_at = -1;
+
+        for (int st = 0; st < nsteps; ++st) {
+            double xin, xout;
+            int gi;
+            if (P.mode == 2) {
+                xin = P.x_in[item];
+                xout = P.x_out[item];
+                gi = 0;
+            } else if (side == 0) {
+                gi = st;
+                xin = P.grid[gi];
+                xout = P.grid[gi + 1];
+            } else {
+                gi = P.nl + P.nr - st;
+                xin = P.grid[gi];
+                xout = P.grid[gi - 1];
+            }
+            const double dx = xout - xin;
+            const double xs = xin + dx * P.c[s];
+
+            bool converged = false;
+            int its_reached = 0;
+            for (int its = 0; its < P.max_its; ++its) {
+                ++its_reached;
+                rhs_eval<N>(ykm, uvm, xs, dim, P.dim_m2_cubed, k0, t, b0, b1, cur, &lam[s], P.twN, sy, active, zero_slot);
+                sy.sync();  // every stage RHS is in shared memory
+                double part = 0.0;
+                if (active) {
+#pragma unroll
+                    for (int sg = 0; sg < 8; ++sg) {
+                        double2 nv = ys[sg * TG + t];
+#pragma unroll
+                        for (int kk = 0; kk < S; ++kk) {
+                            const double w = dx * P.a[s][kk];
+                            const double2 f = ex[(size_t)(kk * 2 + cur) * K::MP + sg * TG + t];
+                            nv.x = fma(w, f.x, nv.x);
+                            nv.y = fma(w, f.y, nv.y);
+                        }
+                        const double2 old = ykm[sg * TG + t];
+                        const double ex_ = old.x - nv.x, ey_ = old.y - nv.y;
+                        part = fma(ex_, ex_, part);
+                        part = fma(ey_, ey_, part);
+                        ykm[sg * TG + t] = nv;
+                    }
+                }
+                const double tot = sweep_sum<STP, K::NW>(part, red, lt, sy);
+                const double norm2 = sqrt(tot / (double)(N * S));
+                double p10 = P.prec;
+                if (its > P.max_its / 2) p10 = P.prec * 10.0 * (2.0 * (double)its / (double)P.max_its - 0.5);
+                if (norm2 < p10) {
+                    converged = true;
+                    break;
+                }
+                if constexpr (K::NW == 1) sy.sync();  // new stage values visible to every lane
+            }
+            n_its += its_reached;
+            n_steps += 1;
+            // y += dx sum_i b_i f_i with the RHS of the last evaluation; stages restart at y
+            if (active) {
+#pragma unroll
+                for (int sg = 0; sg < 8; ++sg) {
+                    double2 y = ys[sg * TG + t];
+#pragma unroll
+                    for (int i = 0; i < S; ++i) {
+                        const double w = dx * P.b[i];
+                        const double2 f = ex[(size_t)(i * 2 + cur) * K::MP + sg * TG + t];
+                        y.x = fma(w, f.x, y.x);
+                        y.y = fma(w, f.y, y.y);
+                    }
+                    ykm[sg * TG + t] = y;
+                }
+            }
+            sy.sync();  // every group has read the old y
+            if (active && s == 0) {
+#pragma unroll
+                for (int sg = 0; sg < 8; ++sg) ys[sg * TG + t] = ykm[sg * TG + t];
+            }
+            if (P.mode == 2 && active && s == 0 && t == 0 && P.its_out) P.its_out[item] = its_reached;
+            if (!converged) {
+                status = 1;
+                fail_at = gi;
+                break;
+            }
+        }
+        // write the final state
+        if (active && s == 0) {
+            double* yo = P.yfinal + (size_t)item * N;
+#pragma unroll
+            for (int sg = 0; sg < 8; ++sg) {
+                const int m = slot_mode<N>(sg, t);
+                const double2 y = ys[sg * TG + t];
+                yo[2 * m] = y.x;
+                yo[2 * m + 1] = y.y;
+            }
+            if (t == 0) {
+                P.status[item] = status;
+                P.fail_index[item] = fail_at;
+            }
+        }
+        sy.sync();
+    }
+    if (lt == 0 && P.counters) {
+        atomicAdd(&P.counters[0], n_its * (unsigned long long)S);
+        atomicAdd(&P.counters[1], n_its);
+        atomicAdd(&P.counters[2], n_steps);
+    }
+}
+
+}  // namespace pcc

@@ -1,0 +1,790 @@
+// pcc_abi.cu -- the C ABI of include/pcc.h over the CUDA kernels.
+//
+// A Jacobian build (NewtonSolver::assembleJacobian, NewtonSolver.cpp:615-702)
+// is one stream-ordered pipeline over columns [c0, c1):
+//   1. prologue : per (column, side) unpack + Taylor expansion  -> y_init
+//   2. march    : ONE persistent launch over all 2*(c1-c0) sweeps -> y_final
+//   3. epilogue : per column mismatch, fields, pack               -> out_c
+//   4. fd       : J[:, c] = (out_c - out0) / eps (tiled transpose)
+// Column index Nnewton denotes the unperturbed base shoot.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pcc.h"
+#include "pcc_internal.h"
+
+using namespace pcc;
+
+struct pcc_ctx {
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    // LU workspace (grown on demand)
+    void* lu_work = nullptr;
+    size_t lu_work_bytes = 0;
+};
+
+struct pcc_solve {
+    pcc_ctx* ctx = nullptr;
+    pcc_solve_desc d{};
+    int nn = 0;      // Nnewton
+    int ngrid = 0;   // nl + nr + 1
+    int stages = 2;
+    double a[3][3]{}, b[3]{}, c[3]{};
+    double dm2c = 0.0;
+    std::vector<double> grid;
+    // device buffers
+    double* d_grid = nullptr;
+    double2* d_tw = nullptr;
+    double* d_in0 = nullptr;
+    double* d_out0 = nullptr;
+    double* d_J = nullptr;
+    double* d_yinit = nullptr;    // [2*(nn+1)][N]
+    double* d_yfinal = nullptr;   // [2*(nn+1)][N]
+    double* d_outc = nullptr;     // [nn+1][nn]
+    int* d_status = nullptr;      // [2*(nn+1)] march status
+    int* d_fail = nullptr;        // [2*(nn+1)]
+    int* d_cstatus = nullptr;     // [nn+1] epilogue status
+    int* d_counters_i = nullptr;  // [4] work counters
+    unsigned long long* d_counters = nullptr;  // [4] march counters
+    double* d_scratch = nullptr;
+    int scratch_ctas = 0;
+    int* d_item_side = nullptr;   // pcc_sweep
+    double* d_xs = nullptr;       // pcc_sweep / test entry points (x_in, x_out)
+    int* d_its = nullptr;
+    // last asynchronous build
+    int pend_c0 = 0, pend_c1 = 0;
+    bool pending = false;
+    cudaEvent_t ev[5]{};
+    MarchLaunchInfo last_launch{};
+};
+
+namespace {
+
+const char* kStatusNames[] = {"PCC_OK",
+                              "PCC_ERR_INVALID_ARG",
+                              "PCC_ERR_CUDA",
+                              "PCC_ERR_OOM",
+                              "PCC_ERR_IRK_NO_CONVERGENCE",
+                              "PCC_ERR_DELTA_MISMATCH",
+                              "PCC_ERR_NAN",
+                              "PCC_ERR_LU_SINGULAR",
+                              "PCC_ERR_IR_STALL",
+                              "PCC_ERR_UNSUPPORTED",
+                              "PCC_ERR_NEWTON_NO_CONVERGENCE",
+                              "PCC_ERR_BUSY"};
+
+pcc_status fail(pcc_ctx* ctx, pcc_status s, const std::string& msg)
+{
+    if (ctx) ctx->last_error = msg;
+    return s;
+}
+
+#define PCC_CUDA(ctx, call)                                                                          \
+    do {                                                                                             \
+        cudaError_t _e = (call);                                                                     \
+        if (_e != cudaSuccess) {                                                                     \
+            return fail((ctx), _e == cudaErrorMemoryAllocation ? PCC_ERR_OOM : PCC_ERR_CUDA,         \
+                        std::string(#call) + ": " + cudaGetErrorString(_e));                         \
+        }                                                                                            \
+    } while (0)
+
+// Gauss-Legendre tableaux exactly as ODEStepper.cpp:27-79 builds them.
+int tableau(int scheme, double a[3][3], double b[3], double c[3])
+{
+    for (int i = 0; i < 3; ++i) {
+        b[i] = c[i] = 0.0;
+        for (int j = 0; j < 3; ++j) a[i][j] = 0.0;
+    }
+    if (scheme == 1) {
+        a[0][0] = 0.5;
+        b[0] = 1.0;
+        c[0] = 0.5;
+        return 1;
+    }
+    if (scheme == 3) {
+        a[0][0] = 5.0 / 36.0;
+        a[0][1] = 2.0 / 9.0 - 1.0 / std::sqrt(15.0);
+        a[0][2] = 5.0 / 36.0 - 0.5 / std::sqrt(15.0);
+        a[1][0] = 5.0 / 36.0 + std::sqrt(15.0) / 24.0;
+        a[1][1] = 2.0 / 9.0;
+        a[1][2] = 5.0 / 36.0 - std::sqrt(15.0) / 24.0;
+        a[2][0] = 5.0 / 36.0 + 0.5 / std::sqrt(15.0);
+        a[2][1] = 2.0 / 9.0 + 1.0 / std::sqrt(15.0);
+        a[2][2] = 5.0 / 36.0;
+        b[0] = b[2] = 5.0 / 18.0;
+        b[1] = 4.0 / 9.0;
+        c[0] = 0.5 - std::sqrt(15.0) / 10.0;
+        c[1] = 0.5;
+        c[2] = 0.5 + std::sqrt(15.0) / 10.0;
+        return 3;
+    }
+    a[0][0] = 0.25;
+    a[0][1] = 0.25 - 0.5 / std::sqrt(3.0);
+    a[1][0] = 0.25 + 0.5 / std::sqrt(3.0);
+    a[1][1] = 0.25;
+    b[0] = b[1] = 0.5;
+    c[0] = 0.5 - 0.5 / std::sqrt(3.0);
+    c[1] = 0.5 + 0.5 / std::sqrt(3.0);
+    return 2;
+}
+
+// exp(+2 pi i k/n), k < n, rounded from long-double trigonometry
+std::vector<double2> twiddles(int n)
+{
+    std::vector<double2> tw(n);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int k = 0; k < n; ++k) {
+        const long double a = two_pi * (long double)k / (long double)n;
+        tw[k] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    return tw;
+}
+
+// NewtonSolver::generateGrid (NewtonSolver.cpp:477-519): uniform in logit x.
+// This runs once per solve on the host, as the reference's driver does.
+void make_grid(const pcc_solve_desc& d, std::vector<double>& g)
+{
+    const int il = 0, im = d.nl, ir = d.nl + d.nr;
+    g.assign(ir + 1, 0.0);
+    g[il] = d.xl;
+    g[im] = d.xm;
+    g[ir] = d.xr;
+    const double zl = std::log(d.xl) - std::log(1.0 - d.xl);
+    const double zm = std::log(d.xm) - std::log(1.0 - d.xm);
+    const double zr = std::log(d.xr) - std::log(1.0 - d.xr);
+    const double dzl = (zm - zl) / (double)d.nl;
+    const double dzr = (zr - zm) / (double)d.nr;
+    for (int j = il + 1; j < im; ++j) {
+        const double e = zl + (double)(j - il) * dzl;
+        g[j] = std::exp(e) / (1.0 + std::exp(e));
+    }
+    for (int j = im + 1; j < ir; ++j) {
+        const double e = zm + (double)(j - im) * dzr;
+        g[j] = std::exp(e) / (1.0 + std::exp(e));
+    }
+}
+
+bool desc_ok(const pcc_solve_desc* d, std::string& why)
+{
+    if (!d) return why = "null descriptor", false;
+    if (!march_supported(d->ntau, d->scheme)) return why = "Ntau must be 128..2048 (power of two), scheme 1..3", false;
+    if (d->nl < 1 || d->nr < 1) return why = "NLeft and NRight must be positive", false;
+    if (!(d->xl > 0.0 && d->xl < d->xm && d->xm < d->xr && d->xr < 1.0)) return why = "need 0 < XLeft < XMid < XRight < 1", false;
+    if (!(d->eps_newton > 0.0)) return why = "EpsNewton must be positive", false;
+    if (d->max_irk < 1) return why = "MaxIterIRK must be positive", false;
+    if (!std::isfinite(d->dim) || d->dim <= 2.0) return why = "Dim must be finite and > 2", false;
+    return true;
+}
+
+int boundary_ctas(pcc_solve* s, int items)
+{
+    int c = s->scratch_ctas;
+    return items < c ? items : c;
+}
+
+MarchParams march_params(pcc_solve* s)
+{
+    MarchParams P{};
+    P.grid = s->d_grid;
+    P.nl = s->d.nl;
+    P.nr = s->d.nr;
+    P.dim = s->d.dim;
+    P.dim_m2_cubed = s->dm2c;
+    P.prec = s->d.prec_irk;
+    P.max_its = s->d.max_irk;
+    P.stages = s->stages;
+    for (int i = 0; i < 3; ++i) {
+        P.b[i] = s->b[i];
+        P.c[i] = s->c[i];
+        for (int j = 0; j < 3; ++j) P.a[i][j] = s->a[i][j];
+    }
+    P.twN = s->d_tw;
+    P.status = s->d_status;
+    P.fail_index = s->d_fail;
+    P.counters = s->d_counters;
+    return P;
+}
+
+// Enqueues the build pipeline for columns [c0, c1) reading d_in0 (and d_out0
+// for the differences when fd is set).  Events bracket the stages.
+pcc_status enqueue_columns(pcc_solve* s, int c0, int c1, bool fd, double* d_J)
+{
+    pcc_ctx* ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    const int ncols = c1 - c0;
+    const int items = 2 * ncols;
+    PCC_CUDA(ctx, cudaMemsetAsync(s->d_counters_i, 0, 4 * sizeof(int), st));
+    PCC_CUDA(ctx, cudaMemsetAsync(s->d_counters, 0, 4 * sizeof(unsigned long long), st));
+    PCC_CUDA(ctx, cudaEventRecord(s->ev[0], st));
+
+    BoundaryParams B{};
+    B.ntau = s->d.ntau;
+    B.nn = s->nn;
+    B.c0 = c0;
+    B.dim = s->d.dim;
+    B.xl = s->d.xl;
+    B.xr = s->d.xr;
+    B.eps = s->d.eps_newton;
+    B.prec = s->d.prec_irk;
+    B.dim_m2_cubed = s->dm2c;
+    B.in0 = s->d_in0;
+    B.out0 = s->d_out0;
+    B.yinit = s->d_yinit;
+    B.yfinal = s->d_yfinal;
+    B.outc = s->d_outc;
+    B.status = s->d_cstatus;
+    B.scratch = s->d_scratch;
+    B.tw = s->d_tw;
+
+    B.n_items = items;
+    B.work_counter = s->d_counters_i + 0;
+    PCC_CUDA(ctx, launch_prologue(B, boundary_ctas(s, items), st));
+    PCC_CUDA(ctx, cudaEventRecord(s->ev[1], st));
+
+    MarchParams P = march_params(s);
+    P.n_items = items;
+    P.mode = 0;
+    P.yinit = s->d_yinit;
+    P.yfinal = s->d_yfinal;
+    P.work_counter = s->d_counters_i + 1;
+    PCC_CUDA(ctx, launch_march(s->d.ntau, s->stages, P, 0, st, &s->last_launch));
+    PCC_CUDA(ctx, cudaEventRecord(s->ev[2], st));
+
+    B.n_items = ncols;
+    B.work_counter = s->d_counters_i + 2;
+    PCC_CUDA(ctx, launch_epilogue(B, boundary_ctas(s, ncols), st));
+    if (fd) {
+        // columns [c0, min(c1, nn)) of J; the base column (index nn) has no difference
+        const int nfd = (c1 > s->nn ? s->nn : c1) - c0;
+        if (nfd > 0) PCC_CUDA(ctx, launch_fd(s->d_outc, s->d_out0, d_J, s->nn, c0, nfd, s->d.eps_newton, st));
+    }
+    PCC_CUDA(ctx, cudaEventRecord(s->ev[3], st));
+    return PCC_OK;
+}
+
+// Reads statuses and counters of the last build (synchronises the stream).
+pcc_status collect(pcc_solve* s, int c0, int c1, pcc_stats* stats)
+{
+    pcc_ctx* ctx = s->ctx;
+    PCC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const int ncols = c1 - c0;
+    std::vector<int> st(2 * ncols), fi(2 * ncols), cs(ncols);
+    unsigned long long cnt[4] = {0, 0, 0, 0};
+    PCC_CUDA(ctx, cudaMemcpy(st.data(), s->d_status, st.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    PCC_CUDA(ctx, cudaMemcpy(fi.data(), s->d_fail, fi.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    PCC_CUDA(ctx, cudaMemcpy(cs.data(), s->d_cstatus, cs.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    PCC_CUDA(ctx, cudaMemcpy(cnt, s->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+    pcc_status result = PCC_OK;
+    int fcol = -1, fside = 0, fidx = -1;
+    for (int i = 0; i < 2 * ncols && result == PCC_OK; ++i)
+        if (st[i] != 0) {
+            result = PCC_ERR_IRK_NO_CONVERGENCE;
+            fcol = c0 + i / 2;
+            fside = i & 1;
+            fidx = fi[i];
+        }
+    for (int i = 0; i < ncols && result == PCC_OK; ++i)
+        if (cs[i] != 0) {
+            result = PCC_ERR_DELTA_MISMATCH;
+            fcol = c0 + i;
+        }
+    if (stats) {
+        float ms[3] = {0, 0, 0};
+        cudaEventElapsedTime(&ms[0], s->ev[0], s->ev[1]);
+        cudaEventElapsedTime(&ms[1], s->ev[1], s->ev[2]);
+        cudaEventElapsedTime(&ms[2], s->ev[2], s->ev[3]);
+        stats->rhs_evals = (long long)cnt[0];
+        stats->irk_iterations = (long long)cnt[1];
+        stats->irk_steps = (long long)cnt[2];
+        stats->shoots = ncols;
+        stats->ms_prologue = ms[0];
+        stats->ms_sweep = ms[1];
+        stats->ms_epilogue = ms[2];
+        stats->ms_total = (double)ms[0] + ms[1] + ms[2];
+        stats->fail_column = fcol;
+        stats->fail_side = fside;
+        stats->fail_grid_index = fidx;
+        stats->sweep_ctas = s->last_launch.ctas;
+    }
+    if (result != PCC_OK) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "%s at column %d side %d grid index %d", kStatusNames[result], fcol, fside, fidx);
+        ctx->last_error = buf;
+    }
+    return result;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pcc_status_string(pcc_status s)
+{
+    const int i = (int)s;
+    return (i >= 0 && i < (int)(sizeof(kStatusNames) / sizeof(kStatusNames[0]))) ? kStatusNames[i] : "PCC_UNKNOWN";
+}
+
+const char* pcc_last_error(pcc_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+pcc_status pcc_ctx_create(int device, const pcc_ctx_opts* opts, pcc_ctx** out)
+{
+    if (!out) return PCC_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (opts && opts->reserved != 0) return PCC_ERR_INVALID_ARG;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return PCC_ERR_CUDA;
+    auto* ctx = new pcc_ctx;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return PCC_ERR_CUDA;
+    }
+    *out = ctx;
+    return PCC_OK;
+}
+
+pcc_status pcc_ctx_destroy(pcc_ctx* ctx)
+{
+    if (!ctx) return PCC_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->lu_work) cudaFree(ctx->lu_work);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return PCC_OK;
+}
+
+pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve** out)
+{
+    if (!ctx || !out) return PCC_ERR_INVALID_ARG;
+    *out = nullptr;
+    std::string why;
+    if (!desc_ok(desc, why)) return fail(ctx, PCC_ERR_INVALID_ARG, why);
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    auto* s = new pcc_solve;
+    s->ctx = ctx;
+    s->d = *desc;
+    s->nn = 3 * desc->ntau / 4;
+    s->ngrid = desc->nl + desc->nr + 1;
+    s->stages = tableau(desc->scheme, s->a, s->b, s->c);
+    s->dm2c = std::pow(desc->dim - 2.0, 3);
+    make_grid(*desc, s->grid);
+    const int n = desc->ntau, nn = s->nn, cols = nn + 1;
+    s->scratch_ctas = 2 * ctx->sms;
+    auto cleanup = [&](pcc_status st, const std::string& m) {
+        pcc_solve_destroy(s);
+        return fail(ctx, st, m);
+    };
+#define ALLOC(ptr, bytes)                                                                                    \
+    do {                                                                                                     \
+        cudaError_t _e = cudaMalloc((void**)&(ptr), (bytes));                                                \
+        if (_e != cudaSuccess) return cleanup(PCC_ERR_OOM, std::string("cudaMalloc ") + #ptr + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+    ALLOC(s->d_grid, s->ngrid * sizeof(double));
+    ALLOC(s->d_tw, n * sizeof(double2));
+    ALLOC(s->d_in0, nn * sizeof(double));
+    ALLOC(s->d_out0, nn * sizeof(double));
+    ALLOC(s->d_J, (size_t)nn * nn * sizeof(double));
+    ALLOC(s->d_yinit, (size_t)2 * cols * n * sizeof(double));
+    ALLOC(s->d_yfinal, (size_t)2 * cols * n * sizeof(double));
+    ALLOC(s->d_outc, (size_t)cols * nn * sizeof(double));
+    ALLOC(s->d_status, 2 * cols * sizeof(int));
+    ALLOC(s->d_fail, 2 * cols * sizeof(int));
+    ALLOC(s->d_cstatus, cols * sizeof(int));
+    ALLOC(s->d_counters_i, 4 * sizeof(int));
+    ALLOC(s->d_counters, 4 * sizeof(unsigned long long));
+    ALLOC(s->d_scratch, (size_t)s->scratch_ctas * kBoundaryArrays * n * sizeof(double));
+    ALLOC(s->d_item_side, 2 * cols * sizeof(int));
+    ALLOC(s->d_xs, 4 * cols * sizeof(double));
+    ALLOC(s->d_its, 2 * cols * sizeof(int));
+#undef ALLOC
+    const std::vector<double2> tw = twiddles(n);
+    cudaError_t e = cudaMemcpy(s->d_tw, tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->d_grid, s->grid.data(), s->ngrid * sizeof(double), cudaMemcpyHostToDevice);
+    for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&s->ev[i]);
+    if (e != cudaSuccess) return cleanup(PCC_ERR_CUDA, cudaGetErrorString(e));
+    *out = s;
+    return PCC_OK;
+}
+
+pcc_status pcc_solve_destroy(pcc_solve* s)
+{
+    if (!s) return PCC_ERR_INVALID_ARG;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    void* ptrs[] = {s->d_grid, s->d_tw, s->d_in0, s->d_out0, s->d_J, s->d_yinit, s->d_yfinal, s->d_outc,
+                    s->d_status, s->d_fail, s->d_cstatus, s->d_counters_i, s->d_counters, s->d_scratch,
+                    s->d_item_side, s->d_xs, s->d_its};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (auto& ev : s->ev)
+        if (ev) cudaEventDestroy(ev);
+    delete s;
+    return PCC_OK;
+}
+
+pcc_status pcc_solve_grid(pcc_solve* s, double* grid_out)
+{
+    if (!s || !grid_out) return PCC_ERR_INVALID_ARG;
+    std::memcpy(grid_out, s->grid.data(), s->grid.size() * sizeof(double));
+    return PCC_OK;
+}
+
+pcc_status pcc_jacobian_columns(pcc_solve* s, const double* in0, const double* out0, int c0, int c1, double* cols,
+                                pcc_stats* stats)
+{
+    if (!s || !in0 || !cols) return PCC_ERR_INVALID_ARG;
+    if (c0 < 0 || c1 > s->nn + 1 || c0 >= c1) return fail(s->ctx, PCC_ERR_INVALID_ARG, "column range");
+    const bool base_only = (c0 == s->nn);
+    if (!base_only && !out0) return PCC_ERR_INVALID_ARG;
+    pcc_ctx* ctx = s->ctx;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int nn = s->nn;
+    PCC_CUDA(ctx, cudaMemcpyAsync(s->d_in0, in0, nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if (out0) PCC_CUDA(ctx, cudaMemcpyAsync(s->d_out0, out0, nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    pcc_status r = enqueue_columns(s, c0, c1, false, nullptr);
+    if (r != PCC_OK) return r;
+    // columns as differences (or the raw packed output for the base column)
+    const int ncols = c1 - c0;
+    std::vector<double> outc((size_t)ncols * nn), o0(nn);
+    PCC_CUDA(ctx, cudaMemcpyAsync(outc.data(), s->d_outc, outc.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    r = collect(s, c0, c1, stats);
+    for (int i = 0; i < ncols; ++i) {
+        const int col = c0 + i;
+        for (int j = 0; j < nn; ++j) {
+            const double v = outc[(size_t)i * nn + j];
+            cols[(size_t)i * nn + j] = (col == nn) ? v : (v - out0[j]) / s->d.eps_newton;
+        }
+    }
+    return r;
+}
+
+pcc_status pcc_shoot(pcc_solve* s, const double* in0, double* out0, pcc_stats* stats)
+{
+    if (!s || !in0 || !out0) return PCC_ERR_INVALID_ARG;
+    return pcc_jacobian_columns(s, in0, nullptr, s->nn, s->nn + 1, out0, stats);
+}
+
+pcc_status pcc_jacobian_device(pcc_solve* s, const double* d_in0, const double* d_out0, double* d_J)
+{
+    if (!s || !d_in0 || !d_out0 || !d_J) return PCC_ERR_INVALID_ARG;
+    pcc_ctx* ctx = s->ctx;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int nn = s->nn;
+    if (d_in0 != s->d_in0)
+        PCC_CUDA(ctx, cudaMemcpyAsync(s->d_in0, d_in0, nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    if (d_out0 != s->d_out0)
+        PCC_CUDA(ctx, cudaMemcpyAsync(s->d_out0, d_out0, nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    pcc_status r = enqueue_columns(s, 0, nn, true, d_J);
+    if (r != PCC_OK) return r;
+    s->pend_c0 = 0;
+    s->pend_c1 = nn;
+    s->pending = true;
+    return PCC_OK;
+}
+
+pcc_status pcc_solve_sync(pcc_solve* s, pcc_stats* stats)
+{
+    if (!s) return PCC_ERR_INVALID_ARG;
+    if (!s->pending) {
+        cudaStreamSynchronize(s->ctx->stream);
+        return PCC_OK;
+    }
+    s->pending = false;
+    return collect(s, s->pend_c0, s->pend_c1, stats);
+}
+
+pcc_status pcc_jacobian(pcc_solve* s, const double* in0, const double* out0, double* J, pcc_stats* stats)
+{
+    if (!s || !in0 || !out0 || !J) return PCC_ERR_INVALID_ARG;
+    pcc_ctx* ctx = s->ctx;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int nn = s->nn;
+    PCC_CUDA(ctx, cudaMemcpyAsync(s->d_in0, in0, nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    PCC_CUDA(ctx, cudaMemcpyAsync(s->d_out0, out0, nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    pcc_status r = enqueue_columns(s, 0, nn, true, s->d_J);
+    if (r != PCC_OK) return r;
+    PCC_CUDA(ctx, cudaMemcpyAsync(J, s->d_J, (size_t)nn * nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    return collect(s, 0, nn, stats);
+}
+
+pcc_status pcc_boundary_data(pcc_solve* s, const double* in0, double* y_left, double* y_right)
+{
+    if (!s || !in0 || !y_left || !y_right) return PCC_ERR_INVALID_ARG;
+    pcc_ctx* ctx = s->ctx;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int nn = s->nn, n = s->d.ntau;
+    PCC_CUDA(ctx, cudaMemcpyAsync(s->d_in0, in0, nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    PCC_CUDA(ctx, cudaMemsetAsync(s->d_counters_i, 0, 4 * sizeof(int), ctx->stream));
+    BoundaryParams B{};
+    B.ntau = n;
+    B.nn = nn;
+    B.c0 = nn;  // base column: no perturbation
+    B.dim = s->d.dim;
+    B.xl = s->d.xl;
+    B.xr = s->d.xr;
+    B.eps = s->d.eps_newton;
+    B.in0 = s->d_in0;
+    B.yinit = s->d_yinit;
+    B.scratch = s->d_scratch;
+    B.tw = s->d_tw;
+    B.n_items = 2;
+    B.work_counter = s->d_counters_i;
+    PCC_CUDA(ctx, launch_prologue(B, 2, ctx->stream));
+    PCC_CUDA(ctx, cudaMemcpyAsync(y_left, s->d_yinit, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PCC_CUDA(ctx, cudaMemcpyAsync(y_right, s->d_yinit + n, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PCC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PCC_OK;
+}
+
+pcc_status pcc_sweep(pcc_solve* s, int count, const int* sides, const double* y_init, double* y_final,
+                     pcc_stats* stats)
+{
+    if (!s || count < 1 || !sides || !y_init || !y_final) return PCC_ERR_INVALID_ARG;
+    if (count > 2 * (s->nn + 1)) return fail(s->ctx, PCC_ERR_INVALID_ARG, "too many sweeps for this solve");
+    pcc_ctx* ctx = s->ctx;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int n = s->d.ntau;
+    cudaStream_t st = ctx->stream;
+    PCC_CUDA(ctx, cudaMemcpyAsync(s->d_yinit, y_init, (size_t)count * n * sizeof(double), cudaMemcpyHostToDevice, st));
+    PCC_CUDA(ctx, cudaMemcpyAsync(s->d_item_side, sides, count * sizeof(int), cudaMemcpyHostToDevice, st));
+    PCC_CUDA(ctx, cudaMemsetAsync(s->d_counters_i, 0, 4 * sizeof(int), st));
+    PCC_CUDA(ctx, cudaMemsetAsync(s->d_counters, 0, 4 * sizeof(unsigned long long), st));
+    MarchParams P = march_params(s);
+    P.n_items = count;
+    P.mode = 0;
+    P.yinit = s->d_yinit;
+    P.yfinal = s->d_yfinal;
+    P.item_side = s->d_item_side;
+    P.work_counter = s->d_counters_i;
+    PCC_CUDA(ctx, cudaEventRecord(s->ev[1], st));
+    PCC_CUDA(ctx, launch_march(n, s->stages, P, 0, st, &s->last_launch));
+    PCC_CUDA(ctx, cudaEventRecord(s->ev[2], st));
+    PCC_CUDA(ctx, cudaMemcpyAsync(y_final, s->d_yfinal, (size_t)count * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PCC_CUDA(ctx, cudaStreamSynchronize(st));
+    std::vector<int> stv(count), fi(count);
+    unsigned long long cnt[4];
+    PCC_CUDA(ctx, cudaMemcpy(stv.data(), s->d_status, count * sizeof(int), cudaMemcpyDeviceToHost));
+    PCC_CUDA(ctx, cudaMemcpy(fi.data(), s->d_fail, count * sizeof(int), cudaMemcpyDeviceToHost));
+    PCC_CUDA(ctx, cudaMemcpy(cnt, s->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+    pcc_status r = PCC_OK;
+    int fcol = -1, fidx = -1, fside = 0;
+    for (int i = 0; i < count; ++i)
+        if (stv[i]) {
+            r = PCC_ERR_IRK_NO_CONVERGENCE;
+            fcol = i;
+            fside = sides[i];
+            fidx = fi[i];
+            break;
+        }
+    if (stats) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, s->ev[1], s->ev[2]);
+        std::memset(stats, 0, sizeof(*stats));
+        stats->rhs_evals = (long long)cnt[0];
+        stats->irk_iterations = (long long)cnt[1];
+        stats->irk_steps = (long long)cnt[2];
+        stats->ms_sweep = ms;
+        stats->ms_total = ms;
+        stats->fail_column = fcol;
+        stats->fail_side = fside;
+        stats->fail_grid_index = fidx;
+        stats->sweep_ctas = s->last_launch.ctas;
+    }
+    return r;
+}
+
+// ODEStepper-level entry points: a temporary solve-less march launch.
+static pcc_status single_states(pcc_ctx* ctx, int ntau, double dim, int scheme, double precision, int max_its,
+                                int count, const double* y, const double* x_in, const double* x_out, double* y_out,
+                                int* its_out, int mode)
+{
+    if (!ctx || count < 1 || !y || !x_in || !y_out || !march_supported(ntau, scheme)) return PCC_ERR_INVALID_ARG;
+    if (mode == 2 && !x_out) return PCC_ERR_INVALID_ARG;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    double *d_y = nullptr, *d_o = nullptr, *d_x = nullptr;
+    double2* d_tw = nullptr;
+    int *d_i = nullptr;
+    unsigned long long* d_c = nullptr;
+    const size_t yb = (size_t)count * ntau * sizeof(double);
+    auto release = [&]() {
+        cudaFree(d_y);
+        cudaFree(d_o);
+        cudaFree(d_x);
+        cudaFree(d_tw);
+        cudaFree(d_i);
+        cudaFree(d_c);
+    };
+    if (cudaMalloc(&d_y, yb) != cudaSuccess || cudaMalloc(&d_o, yb) != cudaSuccess ||
+        cudaMalloc(&d_x, 2 * count * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&d_tw, ntau * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&d_i, (3 * count + 4) * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&d_c, 4 * sizeof(unsigned long long)) != cudaSuccess) {
+        release();
+        return fail(ctx, PCC_ERR_OOM, "allocation for the state batch");
+    }
+    const std::vector<double2> tw = twiddles(ntau);
+    std::vector<double> xs(2 * count);
+    for (int i = 0; i < count; ++i) {
+        xs[i] = x_in[i];
+        xs[count + i] = x_out ? x_out[i] : 0.0;
+    }
+    cudaError_t e = cudaMemcpy(d_y, y, yb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_tw, tw.data(), ntau * sizeof(double2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_x, xs.data(), 2 * count * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(d_i, 0, (3 * count + 4) * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(d_c, 0, 4 * sizeof(unsigned long long));
+    MarchParams P{};
+    double a[3][3], b[3], c[3];
+    const int S = tableau(scheme, a, b, c);
+    P.n_items = count;
+    P.mode = mode;
+    P.yinit = d_y;
+    P.yfinal = d_o;
+    P.dim = dim;
+    P.dim_m2_cubed = std::pow(dim - 2.0, 3);
+    P.prec = precision;
+    P.max_its = max_its;
+    P.stages = S;
+    for (int i = 0; i < 3; ++i) {
+        P.b[i] = b[i];
+        P.c[i] = c[i];
+        for (int j = 0; j < 3; ++j) P.a[i][j] = a[i][j];
+    }
+    P.twN = d_tw;
+    P.x_in = d_x;
+    P.x_out = d_x + count;
+    P.work_counter = d_i + 3 * count;
+    P.status = d_i;
+    P.fail_index = d_i + count;
+    P.its_out = d_i + 2 * count;
+    P.counters = d_c;
+    if (e == cudaSuccess) e = launch_march(ntau, S, P, 0, st, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(y_out, d_o, yb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && its_out) e = cudaMemcpyAsync(its_out, d_i + 2 * count, count * sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    release();
+    if (e != cudaSuccess) return fail(ctx, PCC_ERR_CUDA, cudaGetErrorString(e));
+    return PCC_OK;
+}
+
+pcc_status pcc_rhs_eval(pcc_ctx* ctx, int ntau, double dim, int count, const double* y, const double* x, double* dy)
+{
+    return single_states(ctx, ntau, dim, 2, 1e-15, 1, count, y, x, nullptr, dy, nullptr, 1);
+}
+
+pcc_status pcc_irk_step(pcc_ctx* ctx, int ntau, double dim, int scheme, double precision, int max_its, int count,
+                        const double* y_in, const double* x_in, const double* x_out, double* y_out, int* its_out)
+{
+    if (max_its < 1) return PCC_ERR_INVALID_ARG;
+    return single_states(ctx, ntau, dim, scheme, precision, max_its, count, y_in, x_in, x_out, y_out, its_out, 2);
+}
+
+pcc_status pcc_lu_solve(pcc_ctx* ctx, int n, const double* A, const double* rhs, double* x, pcc_precision prec,
+                        pcc_refine_report* report)
+{
+    if (!ctx || n < 1 || !A || !rhs || !x) return PCC_ERR_INVALID_ARG;
+    if (prec != PCC_PREC_FP64 && prec != PCC_PREC_MIXED) return PCC_ERR_INVALID_ARG;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t nb = (size_t)n * n * sizeof(double);
+    const size_t need = nb + 3 * n * sizeof(double) + 2 * n * sizeof(int) + 16 + lu_mixed_work_bytes(n);
+    if (ctx->lu_work_bytes < need) {
+        if (ctx->lu_work) cudaFree(ctx->lu_work);
+        ctx->lu_work = nullptr;
+        ctx->lu_work_bytes = 0;
+        PCC_CUDA(ctx, cudaMalloc(&ctx->lu_work, need));
+        ctx->lu_work_bytes = need;
+    }
+    char* w = static_cast<char*>(ctx->lu_work);
+    double* dA = reinterpret_cast<double*>(w);
+    double* db = dA + (size_t)n * n;
+    double* dx = db + n;
+    double* dtmp = dx + n;
+    int* ipiv = reinterpret_cast<int*>(dtmp + n);
+    int* info = ipiv + n;
+    void* mixed_work = reinterpret_cast<char*>(info + n) + 16;
+    cudaEvent_t e0, e1;
+    PCC_CUDA(ctx, cudaEventCreate(&e0));
+    PCC_CUDA(ctx, cudaEventCreate(&e1));
+    PCC_CUDA(ctx, cudaMemcpyAsync(dA, A, nb, cudaMemcpyHostToDevice, st));
+    PCC_CUDA(ctx, cudaMemcpyAsync(db, rhs, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    PCC_CUDA(ctx, cudaEventRecord(e0, st));
+    int steps = 0;
+    double resid = -1.0;
+    if (prec == PCC_PREC_FP64) {
+        PCC_CUDA(ctx, lu_solve_fp64(dA, db, dx, n, dtmp, ipiv, info, st));
+    } else {
+        PCC_CUDA(ctx, lu_solve_mixed(dA, db, dx, n, mixed_work, lu_mixed_work_bytes(n), ipiv, info, 30, 1e-15,
+                                     &steps, &resid, st));
+    }
+    PCC_CUDA(ctx, cudaEventRecord(e1, st));
+    int hinfo[2] = {0, 0};
+    PCC_CUDA(ctx, cudaMemcpyAsync(x, dx, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PCC_CUDA(ctx, cudaMemcpyAsync(hinfo, info, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    PCC_CUDA(ctx, cudaStreamSynchronize(st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (report) {
+        report->rel_err_vs_fp64 = -1.0;
+        report->residual_norm = resid;
+        report->refinement_steps = steps;
+        report->fell_back_to_fp64 = hinfo[1];
+        report->ms = ms;
+    }
+    if (hinfo[0] != 0) return fail(ctx, PCC_ERR_LU_SINGULAR, "zero pivot in LU");
+    return PCC_OK;
+}
+
+pcc_status pcc_newton_step(pcc_solve* s, double* in0, double* err_out, pcc_precision prec, pcc_stats* stats,
+                           pcc_refine_report* report)
+{
+    if (!s || !in0) return PCC_ERR_INVALID_ARG;
+    pcc_ctx* ctx = s->ctx;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int nn = s->nn;
+    // base shoot and all Jacobian columns in one pipeline (columns 0..nn)
+    PCC_CUDA(ctx, cudaMemcpyAsync(s->d_in0, in0, nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    pcc_status r = enqueue_columns(s, 0, nn + 1, false, nullptr);
+    if (r != PCC_OK) return r;
+    // out0 = base column output, then J
+    PCC_CUDA(ctx, cudaMemcpyAsync(s->d_out0, s->d_outc + (size_t)nn * nn, nn * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, ctx->stream));
+    PCC_CUDA(ctx, launch_fd(s->d_outc, s->d_out0, s->d_J, nn, 0, nn, s->d.eps_newton, ctx->stream));
+    r = collect(s, 0, nn + 1, stats);
+    if (r != PCC_OK) return r;
+    std::vector<double> out0(nn), J((size_t)nn * nn), rhs(nn), dx(nn);
+    PCC_CUDA(ctx, cudaMemcpy(out0.data(), s->d_out0, nn * sizeof(double), cudaMemcpyDeviceToHost));
+    PCC_CUDA(ctx, cudaMemcpy(J.data(), s->d_J, J.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    double ss = 0.0;
+    for (int i = 0; i < nn; ++i) ss += out0[i] * out0[i];
+    const double err = std::sqrt(ss / (double)nn);  // computeL2Norm (NewtonSolver.cpp:763-768)
+    if (err_out) *err_out = err;
+    for (int i = 0; i < nn; ++i) rhs[i] = -out0[i];
+    r = pcc_lu_solve(ctx, nn, J.data(), rhs.data(), dx.data(), prec, report);
+    if (r != PCC_OK) return r;
+    const double fac = std::min(1.0, s->d.slow_error / err);  // NewtonSolver.cpp:350
+    for (int i = 0; i < nn; ++i) in0[i] += fac * dx[i];       // :358
+    return PCC_OK;
+}
+
+pcc_status pcc_fp64_peak(pcc_ctx* ctx, double* tflops)
+{
+    if (!ctx || !tflops) return PCC_ERR_INVALID_ARG;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    PCC_CUDA(ctx, fp64_peak_probe(tflops, ctx->stream));
+    return PCC_OK;
+}
+
+}  // extern "C"

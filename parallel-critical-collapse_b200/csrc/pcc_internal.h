@@ -1,0 +1,39 @@
+// pcc_internal.h -- declarations shared by the CUDA translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "boundary.cuh"
+#include "march.cuh"
+
+namespace pcc {
+
+cudaError_t launch_prologue(const BoundaryParams& P, int ctas, cudaStream_t st);
+cudaError_t launch_epilogue(const BoundaryParams& P, int ctas, cudaStream_t st);
+cudaError_t launch_fd(const double* outc, const double* out0, double* J, int nn, int c0, int ncols, double eps,
+                      cudaStream_t st);
+
+struct MarchLaunchInfo {
+    int ctas;            // persistent CTAs launched
+    int sweeps_per_cta;  // sweep slots per CTA
+    int threads;         // threads per CTA
+    size_t smem;         // dynamic shared memory per CTA
+    int ctas_per_sm;     // resident CTAs per SM at this shape
+};
+
+// Launches the IRK march for Ntau in {128,...,2048} and 1..3 stages.
+// max_ctas <= 0 means one wave of resident CTAs on every SM.
+cudaError_t launch_march(int ntau, int stages, const MarchParams& P, int max_ctas, cudaStream_t st,
+                         MarchLaunchInfo* info);
+bool march_supported(int ntau, int stages);
+
+// LU helpers (lu.cu)
+cudaError_t lu_solve_fp64(const double* dA, const double* db, double* dx, int n, double* work, int* ipiv,
+                          int* info, cudaStream_t st);
+cudaError_t lu_solve_mixed(const double* dA, const double* db, double* dx, int n, void* work, size_t work_bytes,
+                           int* ipiv, int* info, int max_refine, double tol, int* steps_out, double* resid_out,
+                           cudaStream_t st);
+size_t lu_mixed_work_bytes(int n);
+
+cudaError_t fp64_peak_probe(double* tflops, cudaStream_t st);
+
+}  // namespace pcc

@@ -1,0 +1,290 @@
+"""ctypes binding of include/pcc.h (libpcc_b200.so).
+
+This is how Python callers (the tests, bench.py, a ctypes-based driver) reach
+the CUDA engine.  It loads the in-tree library and raises if it is missing:
+there is no CPU fallback.
+
+    from pcc import Engine, SolveDesc
+    eng = Engine(device=0)
+    solve = eng.solve(SolveDesc.from_config(cfg_dict))
+    out0 = solve.shoot(in0)
+    J = solve.jacobian(in0, out0)
+"""
+import ctypes
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libpcc_b200.so"
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+STATUS = ["PCC_OK", "PCC_ERR_INVALID_ARG", "PCC_ERR_CUDA", "PCC_ERR_OOM", "PCC_ERR_IRK_NO_CONVERGENCE",
+          "PCC_ERR_DELTA_MISMATCH", "PCC_ERR_NAN", "PCC_ERR_LU_SINGULAR", "PCC_ERR_IR_STALL", "PCC_ERR_UNSUPPORTED",
+          "PCC_ERR_NEWTON_NO_CONVERGENCE", "PCC_ERR_BUSY"]
+PREC_FP64, PREC_MIXED = 0, 1
+
+# every function include/pcc.h declares
+EXPORTS = ["pcc_ctx_create", "pcc_ctx_destroy", "pcc_status_string", "pcc_last_error", "pcc_solve_create",
+           "pcc_solve_destroy", "pcc_solve_grid", "pcc_shoot", "pcc_jacobian", "pcc_jacobian_device",
+           "pcc_solve_sync", "pcc_jacobian_columns", "pcc_lu_solve", "pcc_newton_step", "pcc_rhs_eval",
+           "pcc_irk_step", "pcc_boundary_data", "pcc_sweep", "pcc_fp64_peak"]
+
+
+class PccError(RuntimeError):
+    def __init__(self, status, msg):
+        self.status = status
+        self.name = STATUS[status] if 0 <= status < len(STATUS) else str(status)
+        super().__init__(f"{self.name}: {msg}")
+
+
+class SolveDesc(ctypes.Structure):
+    _fields_ = [("ntau", ctypes.c_int), ("dim", ctypes.c_double), ("xl", ctypes.c_double),
+                ("xm", ctypes.c_double), ("xr", ctypes.c_double), ("eps_newton", ctypes.c_double),
+                ("nl", ctypes.c_int), ("nr", ctypes.c_int), ("prec_irk", ctypes.c_double),
+                ("scheme", ctypes.c_int), ("max_irk", ctypes.c_int), ("prec_newton", ctypes.c_double),
+                ("slow_error", ctypes.c_double), ("max_newton", ctypes.c_int)]
+
+    @classmethod
+    def from_config(cls, cfg):
+        """From a reference SimulationConfig dict (include/SimulationConfig.hpp:73-137)."""
+        return cls(int(cfg["Ntau"]), float(cfg["Dim"]), float(cfg["XLeft"]), float(cfg["XMid"]),
+                   float(cfg["XRight"]), float(cfg["EpsNewton"]), int(cfg["NLeft"]), int(cfg["NRight"]),
+                   float(cfg["PrecisionIRK"]), int(cfg["SchemeIRK"]), int(cfg["MaxIterIRK"]),
+                   float(cfg.get("PrecisionNewton", 1e-14)), float(cfg.get("SlowError", 1e-3)),
+                   int(cfg.get("MaxIterNewton", 100)))
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("rhs_evals", ctypes.c_longlong), ("irk_iterations", ctypes.c_longlong),
+                ("irk_steps", ctypes.c_longlong), ("shoots", ctypes.c_longlong), ("ms_prologue", ctypes.c_double),
+                ("ms_sweep", ctypes.c_double), ("ms_epilogue", ctypes.c_double), ("ms_total", ctypes.c_double),
+                ("fail_column", ctypes.c_int), ("fail_side", ctypes.c_int), ("fail_grid_index", ctypes.c_int),
+                ("sweep_ctas", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class RefineReport(ctypes.Structure):
+    _fields_ = [("rel_err_vs_fp64", ctypes.c_double), ("residual_norm", ctypes.c_double),
+                ("refinement_steps", ctypes.c_int), ("fell_back_to_fp64", ctypes.c_int), ("ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def load(path=None):
+    """Loads libpcc_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is missing: run parallel-critical-collapse_b200/build.py")
+    L = ctypes.CDLL(str(p))
+    vp, ci, cd = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    L.pcc_status_string.restype = ctypes.c_char_p
+    L.pcc_status_string.argtypes = [ci]
+    L.pcc_last_error.restype = ctypes.c_char_p
+    L.pcc_last_error.argtypes = [vp]
+    L.pcc_ctx_create.argtypes = [ci, vp, ctypes.POINTER(vp)]
+    L.pcc_ctx_destroy.argtypes = [vp]
+    L.pcc_solve_create.argtypes = [vp, ctypes.POINTER(SolveDesc), ctypes.POINTER(vp)]
+    L.pcc_solve_destroy.argtypes = [vp]
+    L.pcc_solve_grid.argtypes = [vp, _D]
+    L.pcc_shoot.argtypes = [vp, _D, _D, ctypes.POINTER(Stats)]
+    L.pcc_jacobian.argtypes = [vp, _D, _D, _D, ctypes.POINTER(Stats)]
+    L.pcc_jacobian_device.argtypes = [vp, vp, vp, vp]
+    L.pcc_solve_sync.argtypes = [vp, ctypes.POINTER(Stats)]
+    L.pcc_jacobian_columns.argtypes = [vp, _D, _D, ci, ci, _D, ctypes.POINTER(Stats)]
+    L.pcc_lu_solve.argtypes = [vp, ci, _D, _D, _D, ci, ctypes.POINTER(RefineReport)]
+    L.pcc_newton_step.argtypes = [vp, _D, _D, ci, ctypes.POINTER(Stats), ctypes.POINTER(RefineReport)]
+    L.pcc_rhs_eval.argtypes = [vp, ci, cd, ci, _D, _D, _D]
+    L.pcc_irk_step.argtypes = [vp, ci, cd, ci, cd, ci, ci, _D, _D, _D, _D, _I]
+    L.pcc_boundary_data.argtypes = [vp, _D, _D, _D]
+    L.pcc_sweep.argtypes = [vp, ci, _I, _D, _D, ctypes.POINTER(Stats)]
+    L.pcc_fp64_peak.argtypes = [vp, ctypes.POINTER(cd)]
+    for name in EXPORTS:
+        if name not in ("pcc_status_string", "pcc_last_error"):
+            getattr(L, name).restype = ci
+    _lib = L
+    return L
+
+
+def _p(a):
+    return a.ctypes.data_as(_D)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Engine:
+    """A pcc_ctx: one CUDA device and one stream."""
+
+    def __init__(self, device=0):
+        self.lib = load()
+        self.ctx = ctypes.c_void_p()
+        self._check(self.lib.pcc_ctx_create(device, None, ctypes.byref(self.ctx)), ctx=False)
+
+    def _check(self, st, ctx=True):
+        if st != 0:
+            msg = self.lib.pcc_last_error(self.ctx).decode() if ctx and self.ctx else ""
+            raise PccError(st, msg)
+
+    def close(self):
+        if self.ctx:
+            self.lib.pcc_ctx_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, desc):
+        if isinstance(desc, dict):
+            desc = SolveDesc.from_config(desc)
+        return Solve(self, desc)
+
+    def rhs_eval(self, ntau, dim, y, x):
+        y = _f64(y).reshape(-1, ntau)
+        x = _f64(np.atleast_1d(x))
+        out = np.zeros_like(y)
+        self._check(self.lib.pcc_rhs_eval(self.ctx, ntau, dim, y.shape[0], _p(y), _p(x), _p(out)))
+        return out
+
+    def irk_step(self, ntau, dim, scheme, precision, max_its, y, x_in, x_out):
+        y = _f64(y).reshape(-1, ntau)
+        xi = _f64(np.atleast_1d(x_in))
+        xo = _f64(np.atleast_1d(x_out))
+        out = np.zeros_like(y)
+        its = np.zeros(y.shape[0], dtype=np.int32)
+        self._check(self.lib.pcc_irk_step(self.ctx, ntau, dim, scheme, precision, max_its, y.shape[0], _p(y),
+                                          _p(xi), _p(xo), _p(out), its.ctypes.data_as(_I)))
+        return out, its
+
+    def lu_solve(self, A, b, precision=PREC_FP64):
+        A = _f64(A)
+        b = _f64(b)
+        x = np.zeros_like(b)
+        rep = RefineReport()
+        self._check(self.lib.pcc_lu_solve(self.ctx, b.size, _p(A), _p(b), _p(x), precision, ctypes.byref(rep)))
+        return x, rep.as_dict()
+
+    def fp64_peak_tflops(self):
+        v = ctypes.c_double(0)
+        self._check(self.lib.pcc_fp64_peak(self.ctx, ctypes.byref(v)))
+        return v.value
+
+
+class Solve:
+    """A pcc_solve: device buffers, grid and tables for one SimulationConfig."""
+
+    def __init__(self, engine, desc):
+        self.engine = engine
+        self.lib = engine.lib
+        self.desc = desc
+        self.ntau = desc.ntau
+        self.nn = 3 * desc.ntau // 4
+        self.h = ctypes.c_void_p()
+        engine._check(self.lib.pcc_solve_create(engine.ctx, ctypes.byref(desc), ctypes.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            self.lib.pcc_solve_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def grid(self):
+        g = np.zeros(self.desc.nl + self.desc.nr + 1)
+        self.engine._check(self.lib.pcc_solve_grid(self.h, _p(g)))
+        return g
+
+    def shoot(self, in0, stats=None):
+        in0 = _f64(in0)
+        out = np.zeros(self.nn)
+        st = Stats()
+        self.engine._check(self.lib.pcc_shoot(self.h, _p(in0), _p(out), ctypes.byref(st)))
+        if stats is not None:
+            stats.update(st.as_dict())
+        return out
+
+    def jacobian(self, in0, out0, stats=None):
+        in0, out0 = _f64(in0), _f64(out0)
+        J = np.zeros((self.nn, self.nn))
+        st = Stats()
+        self.engine._check(self.lib.pcc_jacobian(self.h, _p(in0), _p(out0), _p(J), ctypes.byref(st)))
+        if stats is not None:
+            stats.update(st.as_dict())
+        return J
+
+    def jacobian_columns(self, in0, out0, c0, c1, stats=None):
+        """Columns [c0, c1) as an (nn, c1-c0) array (column nn = base output)."""
+        in0 = _f64(in0)
+        out0 = _f64(out0) if out0 is not None else None
+        cols = np.zeros((c1 - c0, self.nn))
+        st = Stats()
+        self.engine._check(self.lib.pcc_jacobian_columns(self.h, _p(in0), _p(out0) if out0 is not None else None,
+                                                         c0, c1, _p(cols), ctypes.byref(st)))
+        if stats is not None:
+            stats.update(st.as_dict())
+        return cols.T.copy()
+
+    def jacobian_device(self, d_in0, d_out0, d_J):
+        """Asynchronous build on device pointers (ints); pair with sync()."""
+        self.engine._check(self.lib.pcc_jacobian_device(self.h, ctypes.c_void_p(d_in0), ctypes.c_void_p(d_out0),
+                                                        ctypes.c_void_p(d_J)))
+
+    def sync(self):
+        st = Stats()
+        self.engine._check(self.lib.pcc_solve_sync(self.h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def newton_step(self, in0, precision=PREC_FP64):
+        """One NewtonSolver::run iteration; returns (new in0, err, stats, report)."""
+        x = _f64(in0).copy()
+        err = ctypes.c_double(0)
+        st, rep = Stats(), RefineReport()
+        self.engine._check(self.lib.pcc_newton_step(self.h, _p(x), ctypes.byref(err), precision, ctypes.byref(st),
+                                                    ctypes.byref(rep)))
+        return x, err.value, st.as_dict(), rep.as_dict()
+
+    def boundary_data(self, in0):
+        in0 = _f64(in0)
+        yl, yr = np.zeros(self.ntau), np.zeros(self.ntau)
+        self.engine._check(self.lib.pcc_boundary_data(self.h, _p(in0), _p(yl), _p(yr)))
+        return yl, yr
+
+    def sweep(self, y_init, sides, stats=None):
+        y = _f64(y_init).reshape(-1, self.ntau)
+        sd = np.ascontiguousarray(sides, dtype=np.int32)
+        out = np.zeros_like(y)
+        st = Stats()
+        self.engine._check(self.lib.pcc_sweep(self.h, y.shape[0], sd.ctypes.data_as(_I), _p(y), _p(out),
+                                              ctypes.byref(st)))
+        if stats is not None:
+            stats.update(st.as_dict())
+        return out
+
+
+def config_from_json(path_or_dict):
+    """Loads a reference simulation JSON (dict returned unchanged)."""
+    if isinstance(path_or_dict, dict):
+        return path_or_dict
+    with open(path_or_dict) as f:
+        return json.load(f)

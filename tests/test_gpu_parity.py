@@ -1,0 +1,196 @@
+"""Parity of the CUDA path with the reference (golden fixtures produced by the
+compiled reference) and with the C oracle, through the C ABI.
+
+Tolerances.  All arithmetic is FP64.  RHS, expansions and single IRK steps
+agree to round-off (<= 1e-11 relative; the RHS divides by F - x ~ 1e-3 near
+x = 1).  A shoot returns the ~1e-7 mismatch of O(1) states after thousands of
+steps; two faithful FP64 implementations differ there by ~1e-12 absolute, and
+the finite difference with EpsNewton = 1e-7 turns that into ~1e-5 relative in
+a Jacobian column.  The Newton update itself is checked at the BASELINE
+targets: Delta to 1e-10 relative, free data to 1e-10 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_case, rel_err
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["c1_fixture", "c1_perturbed", "c2_fixture", "c3_fixture"]
+
+
+def _solve(engine, cfg, **over):
+    import pcc
+
+    c = dict(cfg)
+    c.update(over)
+    return engine.solve(pcc.SolveDesc.from_config(c))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_rhs_parity(engine, name):
+    d = load_case(name)
+    cfg = d["cfg"]
+    dy = engine.rhs_eval(cfg["Ntau"], cfg["Dim"], d["rhs_y"], d["rhs_x"])
+    for k, x in enumerate(d["rhs_x"]):
+        assert rel_err(dy[k], d["rhs_dy"][k]) < (1e-10 if x > 0.95 else 1e-12), (name, x)
+
+
+@pytest.mark.parametrize("ntau", [128, 256, 512, 1024, 2048])
+def test_rhs_random_states_vs_oracle(engine, oracle, ntau):
+    """Seeded perturbed states at every supported Ntau, including 256 and 2048."""
+    d = load_case("c1_fixture")
+    cfg = d["cfg"]
+    rng = np.random.default_rng(ntau)
+    # resample the C1 boundary state to ntau modes (zero padding / truncation)
+    base = d["y_left"]
+    y = np.zeros(ntau)
+    m = min(base.size, ntau)
+    y[: m // 2] = base[: m // 2]          # modes 0 .. m/4-1
+    y[ntau - m // 2:] = base[base.size - m // 2:]  # the negative-frequency end
+    y = y * (1 + 1e-3 * rng.standard_normal(ntau))
+    y[4] = base[4]  # Delta
+    xs = np.array([0.002, 0.05, 0.3])
+    dy = engine.rhs_eval(ntau, cfg["Dim"], np.stack([y] * 3), xs)
+    for k, x in enumerate(xs):
+        assert rel_err(dy[k], oracle.rhs(ntau, cfg["Dim"], y, x)) < 1e-12, (ntau, x)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_irk_step_parity(engine, name):
+    d = load_case(name)
+    cfg = d["cfg"]
+    out, its = engine.irk_step(cfg["Ntau"], cfg["Dim"], cfg["SchemeIRK"], cfg["PrecisionIRK"], cfg["MaxIterIRK"],
+                               d["irk_y"], d["irk_x"][:, 0], d["irk_x"][:, 1])
+    for k in range(2):
+        assert rel_err(out[k], d["irk_out"][k]) < 1e-13
+        assert abs(int(its[k]) - int(d["irk_its"][k])) <= 1
+
+
+@pytest.mark.parametrize("scheme", [1, 3])
+def test_irk_schemes_vs_oracle(engine, oracle, scheme):
+    d = load_case("c1_fixture")
+    cfg = d["cfg"]
+    y, xa, xb = d["irk_y"][0], d["irk_x"][0, 0], d["irk_x"][0, 1]
+    out, its = engine.irk_step(128, cfg["Dim"], scheme, 1e-15, 100, y[None], [xa], [xb])
+    ref, k, conv = oracle.irk_step(128, cfg["Dim"], scheme, 1e-15, 100, y, xa, xb)
+    assert conv
+    assert rel_err(out[0], ref) < 1e-13
+    assert abs(int(its[0]) - k) <= 1
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_boundary_data_parity(engine, name):
+    d = load_case(name)
+    s = _solve(engine, d["cfg"])
+    yl, yr = s.boundary_data(d["in0"])
+    assert rel_err(yl, d["y_left"]) < 1e-12
+    assert rel_err(yr, d["y_right"]) < 1e-12
+
+
+def test_grid_parity(engine):
+    d = load_case("c3_fixture")
+    s = _solve(engine, d["cfg"])
+    assert rel_err(s.grid(), d["grid"]) < 1e-15
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_shoot_parity(engine, name):
+    d = load_case(name)
+    s = _solve(engine, d["cfg"])
+    st = {}
+    out0 = s.shoot(d["in0"], stats=st)
+    assert st["rhs_evals"] > 0 and st["fail_column"] == -1
+    # absolute: the outputs are the mismatch itself (~1e-7)
+    assert np.max(np.abs(out0 - d["out0"])) < 1e-10, name
+    assert abs(np.sqrt(np.mean(out0 ** 2)) / np.sqrt(np.mean(d["out0"] ** 2)) - 1) < 1e-3
+
+
+def test_sweep_vs_oracle(engine, oracle):
+    """integrateToMatchPoint of the reference's boundary states, both sides."""
+    d = load_case("c1_fixture")
+    cfg = d["cfg"]
+    s = _solve(engine, cfg)
+    st = {}
+    y = s.sweep(np.stack([d["y_left"], d["y_right"]]), [0, 1], stats=st)
+    yl_o, s0, _, e0 = oracle.sweep(cfg, d["y_left"], True)
+    yr_o, s1, _, e1 = oracle.sweep(cfg, d["y_right"], False)
+    assert s0 == 0 and s1 == 0
+    assert np.max(np.abs(y[0] - yl_o)) < 1e-10
+    assert np.max(np.abs(y[1] - yr_o)) < 1e-10
+    # RHS evaluations counted on the device match the oracle's count closely
+    assert abs(st["rhs_evals"] - (e0 + e1)) <= 0.01 * (e0 + e1)
+
+
+@pytest.mark.parametrize("name", ["c1_fixture", "c1_perturbed"])
+def test_jacobian_c1(engine, name):
+    d = load_case(name)
+    s = _solve(engine, d["cfg"])
+    st = {}
+    J = s.jacobian(d["in0"], d["out0"], stats=st)
+    Jr = d["jac_cols"]
+    errs = [rel_err(J[:, k], Jr[:, k]) for k in range(J.shape[1])]
+    assert max(errs) < 1e-3, max(errs)
+    assert np.median(errs) < 1e-4
+    assert st["shoots"] == 96
+
+
+def test_jacobian_columns_c3(engine):
+    d = load_case("c3_fixture")
+    s = _solve(engine, d["cfg"])
+    c0 = int(d["jac_c0"])
+    cols = s.jacobian_columns(d["in0"], d["out0"], c0, c0 + d["jac_cols"].shape[1])
+    for k in range(cols.shape[1]):
+        assert rel_err(cols[:, k], d["jac_cols"][:, k]) < 1e-3
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_newton_step_c1(engine, precision):
+    """One Newton iteration (NewtonSolver.cpp:298-358) against the reference's."""
+    d = load_case("c1_perturbed")
+    s = _solve(engine, d["cfg"])
+    in1, err, st, rep = s.newton_step(d["in0"], precision=precision)
+    nn = d["in0"].size
+    islot = 2 * nn // 3 + 2
+    assert abs(err / float(d["newton_err"]) - 1) < 1e-3
+    assert abs(in1[islot] / d["newton_in1"][islot] - 1) < 1e-10  # Delta
+    assert np.linalg.norm(in1 - d["newton_in1"]) / np.linalg.norm(d["newton_in1"]) < 1e-10
+    out1 = s.shoot(in1)
+    r1, rr = np.sqrt(np.mean(out1 ** 2)), np.sqrt(np.mean(d["newton_out1"] ** 2))
+    assert r1 < 1.1 * rr + 1e-13
+
+
+def test_lu_fp64_and_mixed(engine):
+    d = load_case("c1_perturbed")
+    J, b = d["jac_cols"], -d["out0"]
+    x64, rep64 = engine.lu_solve(J, b, precision=0)
+    xn = np.linalg.solve(J, b)
+    assert np.linalg.norm(x64 - xn) / np.linalg.norm(xn) < 1e-9
+    xm, repm = engine.lu_solve(J, b, precision=1)
+    assert np.linalg.norm(xm - x64) / np.linalg.norm(x64) < 1e-9
+    assert repm["refinement_steps"] >= 1
+
+
+def test_irk_no_convergence_is_reported(engine):
+    """MaxIterIRK = 1 cannot converge: the reference exits, we return a status."""
+    import pcc
+
+    d = load_case("c1_fixture")
+    s = _solve(engine, d["cfg"], MaxIterIRK=1)
+    with pytest.raises(pcc.PccError) as e:
+        s.shoot(d["in0"])
+    assert e.value.status == 4
+    # the context stays usable
+    s2 = _solve(engine, d["cfg"])
+    out0 = s2.shoot(d["in0"])
+    assert np.max(np.abs(out0 - d["out0"])) < 1e-10
+
+
+def test_invalid_arguments(engine):
+    import pcc
+
+    d = load_case("c1_fixture")
+    for bad in [dict(Ntau=100), dict(NLeft=0), dict(XMid=0.9999), dict(SchemeIRK=4)]:
+        with pytest.raises(pcc.PccError) as e:
+            _solve(engine, d["cfg"], **bad)
+        assert e.value.status == 1
