@@ -94,7 +94,9 @@ typedef struct {
     double ms;
 } pcc_refine_report;
 
-/* Context: one CUDA device, one stream.  NewtonSolver.hpp:150 (ctor) owner. */
+/* Context: one CUDA device, one stream.  NewtonSolver.hpp:150 (ctor) owner.
+ * Destroying a context also destroys the solves still alive in it; their
+ * handles must not be used afterwards. */
 pcc_status pcc_ctx_create(int device, const pcc_ctx_opts* opts, pcc_ctx** out);
 pcc_status pcc_ctx_destroy(pcc_ctx* ctx);
 const char* pcc_status_string(pcc_status s);
@@ -142,7 +144,8 @@ pcc_status pcc_rhs_eval(pcc_ctx* ctx, int ntau, double dim, int count, const dou
                         double* dy);
 
 /* ODEStepper::stepIRK (ODEStepper.cpp:163-292) for `count` independent states
- * (x_in, x_out per state).  its_out (count ints) may be NULL. */
+ * (x_in, x_out per state).  its_out (count ints, may be NULL) receives the
+ * fixed-point iterations used, negated when the step did not converge. */
 pcc_status pcc_irk_step(pcc_ctx* ctx, int ntau, double dim, int scheme, double precision, int max_its, int count,
                         const double* y_in, const double* x_in, const double* x_out, double* y_out, int* its_out);
 
@@ -156,6 +159,29 @@ pcc_status pcc_boundary_data(pcc_solve* s, const double* in0, double* y_left, do
  * x_R -> x_M. */
 pcc_status pcc_sweep(pcc_solve* s, int count, const int* sides, const double* y_init, double* y_final,
                      pcc_stats* stats);
+
+/* computeLeftExpansion / computeRightExpansion from time-domain fields
+ * (InitialConditionGenerator.cpp:37-239, 252-667): y_left from (fc, psic),
+ * y_right from up, at x_l / x_r with period delta.  Pass NULL to skip a side. */
+pcc_status pcc_expansions(pcc_ctx* ctx, int ntau, double dim, double delta, double x_l, double x_r,
+                          const double* fc, const double* psic, const double* up, double* y_left, double* y_right);
+
+/* Replaces the solve's x-grid (NewtonSolver::generateGrid output) by grid,
+ * NLeft + NRight + 1 points, as ShootingSolver::shoot accepts any gridX. */
+pcc_status pcc_solve_set_grid(pcc_solve* s, const double* grid);
+
+/* FFTW-convention DFT of `count` complex series of length n (power of two,
+ * 2..4096), interleaved re/im: out[k] = sum_j in[j] exp(sign 2 pi i jk/n),
+ * unscaled (SpectralTransformer.cpp:22-40 uses sign +1 as "forward"). */
+pcc_status pcc_dft(pcc_ctx* ctx, int n, int count, int sign, const double* in, double* out);
+
+/* InitialConditionGenerator::packSpectralFields / unpackSpectralFields
+ * (InitialConditionGenerator.cpp:678-758): three Ntau-point series <-> the
+ * Nnewton packed Fourier coefficients.  unpack reads z as given (the caller
+ * zeroes the Delta slot as NewtonSolver::shoot does, :408-412). */
+pcc_status pcc_pack_fields(pcc_ctx* ctx, int ntau, const double* up, const double* psic, const double* fc,
+                           double* z);
+pcc_status pcc_unpack_fields(pcc_ctx* ctx, int ntau, const double* z, double* up, double* psic, double* fc);
 
 /* Measured FP64 FMA throughput of this device in TFLOP/s (a short probe). */
 pcc_status pcc_fp64_peak(pcc_ctx* ctx, double* tflops);

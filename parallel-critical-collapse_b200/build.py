@@ -92,9 +92,12 @@ def build_host(force=False):
         return
     lib_srcs = [str(s) for s in srcs if s.name != "main.cpp"]
     cxx = "g++"
-    flags = ["-std=c++17", "-O2", "-fPIC", "-I" + str(REPO / "include"), "-I" + str(HOST)]
+    import sysconfig
+
+    json_inc = Path(sysconfig.get_paths()["purelib"]) / "include" / "cudnn_frontend" / "thirdparty"  # nlohmann/json
+    flags = ["-std=c++17", "-O2", "-fPIC", "-I" + str(REPO / "include"), "-I" + str(HOST), "-I" + str(json_inc)]
     subprocess.run([cxx, "-shared"] + flags + ["-o", str(HOSTLIB)] + lib_srcs +
-                   ["-L" + str(PKG), "-l:libpcc_b200.so", "-Wl,-rpath,$ORIGIN"], check=True)
+                   ["-L" + str(PKG), "-l:libpcc_b200.so", "-Wl,-rpath,$ORIGIN", "-lpthread"], check=True)
     main = HOST / "main.cpp"
     if main.exists():
         subprocess.run([cxx] + flags + ["-o", str(CLI), str(main), "-L" + str(PKG), "-l:libpcc_host.so",

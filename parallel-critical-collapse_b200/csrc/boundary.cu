@@ -437,6 +437,96 @@ __global__ void fd_kernel(const double* __restrict__ outc, const double* __restr
     }
 }
 
+// pack (dir = 0: fields -> z) or unpack (dir = 1: z -> fields), one CTA
+__global__ void __launch_bounds__(256) pack_kernel(int ntau, const double* __restrict__ tw, double* scratch,
+                                                   double* up, double* psic, double* fc, double* z, int dir)
+{
+    extern __shared__ double2 sh[];
+    Blk B;
+    B.n = ntau;
+    B.tw = reinterpret_cast<const double2*>(tw);
+    B.sa = sh;
+    B.sb = sh + ntau;
+    B.scr = scratch;
+    const int nn = 3 * ntau / 4;
+    if (dir == 0) {
+        pack_field(B, up, nn, 0, z);
+        pack_field(B, psic, nn, 1, z);
+        pack_field(B, fc, nn, 2, z);
+    } else {
+        unpack_field(B, z, nn, 0, up);
+        unpack_field(B, z, nn, 1, psic);
+        unpack_field(B, z, nn, 2, fc);
+    }
+}
+
+// expansions from fields (item 0: left from fc/psic, item 1: right from up)
+__global__ void __launch_bounds__(256) expansion_kernel(int ntau, double dim, double delta, double xl, double xr,
+                                                        const double2* __restrict__ tw, double* scratch,
+                                                        const double* fc, const double* psic, const double* up,
+                                                        double* yl, double* yr)
+{
+    extern __shared__ double2 sh[];
+    Blk B;
+    B.n = ntau;
+    B.tw = tw;
+    B.sa = sh;
+    B.sb = sh + ntau;
+    B.scr = scratch + (size_t)blockIdx.x * kBoundaryArrays * ntau;
+    if (blockIdx.x == 0 && yl) left_expansion(B, dim, xl, fc, psic, delta, yl);
+    if (blockIdx.x == 1 && yr) right_expansion(B, dim, xr, up, delta, yr);
+}
+
+cudaError_t launch_expansions(int ntau, double dim, double delta, double xl, double xr, const double2* tw,
+                              double* scratch, const double* fc, const double* psic, const double* up, double* yl,
+                              double* yr, cudaStream_t st)
+{
+    const size_t smem = 2 * (size_t)ntau * sizeof(double2);
+    cudaError_t e = cudaFuncSetAttribute(expansion_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    expansion_kernel<<<2, 256, smem, st>>>(ntau, dim, delta, xl, xr, tw, scratch, fc, psic, up, yl, yr);
+    return cudaGetLastError();
+}
+
+// batched unscaled DFT, one CTA per series
+__global__ void __launch_bounds__(256) dft_kernel(int n, int sign, const double2* __restrict__ tw,
+                                                  const double2* in, double2* out)
+{
+    extern __shared__ double2 sh[];
+    Blk B;
+    B.n = n;
+    B.tw = tw;
+    B.sa = sh;
+    B.sb = sh + n;
+    B.scr = nullptr;
+    const double2* x = in + (size_t)blockIdx.x * n;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) B.sa[j] = x[j];
+    __syncthreads();
+    B.fft(sign);
+    double2* y = out + (size_t)blockIdx.x * n;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) y[j] = B.sa[j];
+}
+
+cudaError_t launch_dft(int n, int count, int sign, const double2* tw, const double2* in, double2* out,
+                       cudaStream_t st)
+{
+    const size_t smem = 2 * (size_t)n * sizeof(double2);
+    cudaError_t e = cudaFuncSetAttribute(dft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dft_kernel<<<count, 256, smem, st>>>(n, sign, tw, in, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack(int ntau, const double2* tw, double* scratch, double* up, double* psic, double* fc, double* z,
+                        int dir, cudaStream_t st)
+{
+    const size_t smem = 2 * (size_t)ntau * sizeof(double2);
+    cudaError_t e = cudaFuncSetAttribute(pack_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    pack_kernel<<<1, 256, smem, st>>>(ntau, reinterpret_cast<const double*>(tw), scratch, up, psic, fc, z, dir);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------ host launchers
 cudaError_t launch_prologue(const BoundaryParams& P, int ctas, cudaStream_t st)
 {

@@ -624,7 +624,8 @@ __global__ void __launch_bounds__(MarchShape<N, S>::NT, MINB) march_kernel(March
 #pragma unroll
                 for (int sg = 0; sg < 8; ++sg) ys[sg * TG + t] = ykm[sg * TG + t];
             }
-            if (P.mode == 2 && active && s == 0 && t == 0 && P.its_out) P.its_out[item] = its_reached;
+            if (P.mode == 2 && active && s == 0 && t == 0 && P.its_out)
+                P.its_out[item] = converged ? its_reached : -its_reached;
             if (!converged) {
                 status = 1;
                 fail_at = gi;

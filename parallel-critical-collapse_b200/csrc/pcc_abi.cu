@@ -9,6 +9,7 @@
 // Column index Nnewton denotes the unperturbed base shoot.
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -23,6 +24,7 @@ struct pcc_ctx {
     int sms = 0;
     cudaStream_t stream = nullptr;
     std::string last_error;
+    std::vector<pcc_solve*> solves;  // live solves; destroyed with the context
     // LU workspace (grown on demand)
     void* lu_work = nullptr;
     size_t lu_work_bytes = 0;
@@ -355,6 +357,7 @@ pcc_status pcc_ctx_destroy(pcc_ctx* ctx)
     if (!ctx) return PCC_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    while (!ctx->solves.empty()) pcc_solve_destroy(ctx->solves.back());
     if (ctx->lu_work) cudaFree(ctx->lu_work);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -410,6 +413,7 @@ pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve*
     if (e == cudaSuccess) e = cudaMemcpy(s->d_grid, s->grid.data(), s->ngrid * sizeof(double), cudaMemcpyHostToDevice);
     for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&s->ev[i]);
     if (e != cudaSuccess) return cleanup(PCC_ERR_CUDA, cudaGetErrorString(e));
+    ctx->solves.push_back(s);
     *out = s;
     return PCC_OK;
 }
@@ -417,6 +421,8 @@ pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve*
 pcc_status pcc_solve_destroy(pcc_solve* s)
 {
     if (!s) return PCC_ERR_INVALID_ARG;
+    auto& v = s->ctx->solves;
+    v.erase(std::remove(v.begin(), v.end(), s), v.end());
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
     void* ptrs[] = {s->d_grid, s->d_tw, s->d_in0, s->d_out0, s->d_J, s->d_yinit, s->d_yfinal, s->d_outc,
@@ -776,6 +782,114 @@ pcc_status pcc_newton_step(pcc_solve* s, double* in0, double* err_out, pcc_preci
     if (r != PCC_OK) return r;
     const double fac = std::min(1.0, s->d.slow_error / err);  // NewtonSolver.cpp:350
     for (int i = 0; i < nn; ++i) in0[i] += fac * dx[i];       // :358
+    return PCC_OK;
+}
+
+static pcc_status pack_common(pcc_ctx* ctx, int ntau, double* up, double* psic, double* fc, double* z, int dir)
+{
+    if (!ctx || !up || !psic || !fc || !z) return PCC_ERR_INVALID_ARG;
+    if (!march_supported(ntau, 2)) return fail(ctx, PCC_ERR_INVALID_ARG, "Ntau must be 128..2048, power of two");
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int nn = 3 * ntau / 4;
+    cudaStream_t st = ctx->stream;
+    double* d = nullptr;
+    const size_t fields = 3 * (size_t)ntau, scr = (size_t)kBoundaryArrays * ntau;
+    const size_t total = fields + nn + scr + 2 * (size_t)ntau;
+    PCC_CUDA(ctx, cudaMalloc(&d, total * sizeof(double)));
+    double *dup = d, *dps = d + ntau, *dfc = d + 2 * ntau, *dz = d + fields, *dscr = dz + nn;
+    double2* dtw = reinterpret_cast<double2*>(dscr + scr);
+    const std::vector<double2> tw = twiddles(ntau);
+    cudaError_t e = cudaMemcpyAsync(dtw, tw.data(), ntau * sizeof(double2), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && dir == 0) {
+        e = cudaMemcpyAsync(dup, up, ntau * sizeof(double), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dps, psic, ntau * sizeof(double), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dfc, fc, ntau * sizeof(double), cudaMemcpyHostToDevice, st);
+    } else if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(dz, z, nn * sizeof(double), cudaMemcpyHostToDevice, st);
+    }
+    if (e == cudaSuccess) e = launch_pack(ntau, dtw, dscr, dup, dps, dfc, dz, dir, st);
+    if (e == cudaSuccess && dir == 0) {
+        e = cudaMemcpyAsync(z, dz, nn * sizeof(double), cudaMemcpyDeviceToHost, st);
+    } else if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(up, dup, ntau * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(psic, dps, ntau * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(fc, dfc, ntau * sizeof(double), cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(ctx, PCC_ERR_CUDA, cudaGetErrorString(e));
+    return PCC_OK;
+}
+
+pcc_status pcc_pack_fields(pcc_ctx* ctx, int ntau, const double* up, const double* psic, const double* fc, double* z)
+{
+    return pack_common(ctx, ntau, const_cast<double*>(up), const_cast<double*>(psic), const_cast<double*>(fc), z, 0);
+}
+
+pcc_status pcc_unpack_fields(pcc_ctx* ctx, int ntau, const double* z, double* up, double* psic, double* fc)
+{
+    return pack_common(ctx, ntau, up, psic, fc, const_cast<double*>(z), 1);
+}
+
+pcc_status pcc_expansions(pcc_ctx* ctx, int ntau, double dim, double delta, double x_l, double x_r,
+                          const double* fc, const double* psic, const double* up, double* y_left, double* y_right)
+{
+    if (!ctx || (!y_left && !y_right) || (y_left && (!fc || !psic)) || (y_right && !up)) return PCC_ERR_INVALID_ARG;
+    if (!march_supported(ntau, 2)) return fail(ctx, PCC_ERR_INVALID_ARG, "Ntau must be 128..2048, power of two");
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t n = ntau, scr = 2 * (size_t)kBoundaryArrays * n;
+    double* d = nullptr;
+    PCC_CUDA(ctx, cudaMalloc(&d, (5 * n + scr + 2 * n) * sizeof(double)));
+    double *dfc = d, *dps = d + n, *dup = d + 2 * n, *dyl = d + 3 * n, *dyr = d + 4 * n, *dscr = d + 5 * n;
+    double2* dtw = reinterpret_cast<double2*>(dscr + scr);
+    const std::vector<double2> tw = twiddles(ntau);
+    cudaError_t e = cudaMemcpyAsync(dtw, tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && y_left) e = cudaMemcpyAsync(dfc, fc, n * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && y_left) e = cudaMemcpyAsync(dps, psic, n * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && y_right) e = cudaMemcpyAsync(dup, up, n * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = launch_expansions(ntau, dim, delta, x_l, x_r, dtw, dscr, dfc, dps, dup, y_left ? dyl : nullptr,
+                              y_right ? dyr : nullptr, st);
+    if (e == cudaSuccess && y_left) e = cudaMemcpyAsync(y_left, dyl, n * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && y_right) e = cudaMemcpyAsync(y_right, dyr, n * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(ctx, PCC_ERR_CUDA, cudaGetErrorString(e));
+    return PCC_OK;
+}
+
+pcc_status pcc_solve_set_grid(pcc_solve* s, const double* grid)
+{
+    if (!s || !grid) return PCC_ERR_INVALID_ARG;
+    for (int i = 1; i < s->ngrid; ++i)
+        if (!(grid[i] > grid[i - 1])) return fail(s->ctx, PCC_ERR_INVALID_ARG, "grid must increase strictly");
+    PCC_CUDA(s->ctx, cudaSetDevice(s->ctx->device));
+    s->grid.assign(grid, grid + s->ngrid);
+    PCC_CUDA(s->ctx, cudaMemcpyAsync(s->d_grid, s->grid.data(), s->ngrid * sizeof(double), cudaMemcpyHostToDevice,
+                                     s->ctx->stream));
+    PCC_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    return PCC_OK;
+}
+
+pcc_status pcc_dft(pcc_ctx* ctx, int n, int count, int sign, const double* in, double* out)
+{
+    if (!ctx || !in || !out || count < 1 || n < 2 || n > 4096 || (n & (n - 1)) || (sign != 1 && sign != -1))
+        return PCC_ERR_INVALID_ARG;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t bytes = (size_t)count * n * sizeof(double2);
+    double2* d = nullptr;
+    PCC_CUDA(ctx, cudaMalloc(&d, 2 * bytes + n * sizeof(double2)));
+    double2* dtw = d + 2 * (size_t)count * n;
+    const std::vector<double2> tw = twiddles(n);
+    cudaError_t e = cudaMemcpyAsync(dtw, tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d, in, bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_dft(n, count, sign, dtw, d, d + (size_t)count * n, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d + (size_t)count * n, bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(ctx, PCC_ERR_CUDA, cudaGetErrorString(e));
     return PCC_OK;
 }
 

@@ -9,6 +9,13 @@ namespace pcc {
 
 cudaError_t launch_prologue(const BoundaryParams& P, int ctas, cudaStream_t st);
 cudaError_t launch_epilogue(const BoundaryParams& P, int ctas, cudaStream_t st);
+cudaError_t launch_pack(int ntau, const double2* tw, double* scratch, double* up, double* psic, double* fc, double* z,
+                        int dir, cudaStream_t st);
+cudaError_t launch_expansions(int ntau, double dim, double delta, double xl, double xr, const double2* tw,
+                              double* scratch, const double* fc, const double* psic, const double* up, double* yl,
+                              double* yr, cudaStream_t st);
+cudaError_t launch_dft(int n, int count, int sign, const double2* tw, const double2* in, double2* out,
+                       cudaStream_t st);
 cudaError_t launch_fd(const double* outc, const double* out0, double* J, int nn, int c0, int ncols, double eps,
                       cudaStream_t st);
 

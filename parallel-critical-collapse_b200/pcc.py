@@ -13,6 +13,7 @@ there is no CPU fallback.
 import ctypes
 import json
 import os
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -32,7 +33,8 @@ PREC_FP64, PREC_MIXED = 0, 1
 EXPORTS = ["pcc_ctx_create", "pcc_ctx_destroy", "pcc_status_string", "pcc_last_error", "pcc_solve_create",
            "pcc_solve_destroy", "pcc_solve_grid", "pcc_shoot", "pcc_jacobian", "pcc_jacobian_device",
            "pcc_solve_sync", "pcc_jacobian_columns", "pcc_lu_solve", "pcc_newton_step", "pcc_rhs_eval",
-           "pcc_irk_step", "pcc_boundary_data", "pcc_sweep", "pcc_fp64_peak"]
+           "pcc_irk_step", "pcc_boundary_data", "pcc_sweep", "pcc_fp64_peak", "pcc_pack_fields",
+           "pcc_unpack_fields", "pcc_expansions", "pcc_solve_set_grid", "pcc_dft"]
 
 
 class PccError(RuntimeError):
@@ -112,6 +114,11 @@ def load(path=None):
     L.pcc_boundary_data.argtypes = [vp, _D, _D, _D]
     L.pcc_sweep.argtypes = [vp, ci, _I, _D, _D, ctypes.POINTER(Stats)]
     L.pcc_fp64_peak.argtypes = [vp, ctypes.POINTER(cd)]
+    L.pcc_pack_fields.argtypes = [vp, ci, _D, _D, _D, _D]
+    L.pcc_unpack_fields.argtypes = [vp, ci, _D, _D, _D, _D]
+    L.pcc_expansions.argtypes = [vp, ci, cd, cd, cd, cd, _D, _D, _D, _D, _D]
+    L.pcc_solve_set_grid.argtypes = [vp, _D]
+    L.pcc_dft.argtypes = [vp, ci, ci, ci, _D, _D]
     for name in EXPORTS:
         if name not in ("pcc_status_string", "pcc_last_error"):
             getattr(L, name).restype = ci
@@ -133,6 +140,7 @@ class Engine:
     def __init__(self, device=0):
         self.lib = load()
         self.ctx = ctypes.c_void_p()
+        self._solves = weakref.WeakSet()
         self._check(self.lib.pcc_ctx_create(device, None, ctypes.byref(self.ctx)), ctx=False)
 
     def _check(self, st, ctx=True):
@@ -141,6 +149,9 @@ class Engine:
             raise PccError(st, msg)
 
     def close(self):
+        """Destroys the context; solves created from it are closed first."""
+        for s in list(self._solves):
+            s.close()
         if self.ctx:
             self.lib.pcc_ctx_destroy(self.ctx)
             self.ctx = ctypes.c_void_p()
@@ -154,7 +165,9 @@ class Engine:
     def solve(self, desc):
         if isinstance(desc, dict):
             desc = SolveDesc.from_config(desc)
-        return Solve(self, desc)
+        s = Solve(self, desc)
+        self._solves.add(s)
+        return s
 
     def rhs_eval(self, ntau, dim, y, x):
         y = _f64(y).reshape(-1, ntau)
@@ -181,6 +194,36 @@ class Engine:
         self._check(self.lib.pcc_lu_solve(self.ctx, b.size, _p(A), _p(b), _p(x), precision, ctypes.byref(rep)))
         return x, rep.as_dict()
 
+    def pack(self, ntau, up, psic, fc):
+        """packSpectralFields(U_p, psi_c, f_c) -> z (Nnewton reals)."""
+        a, b, c = _f64(up), _f64(psic), _f64(fc)
+        z = np.zeros(3 * ntau // 4)
+        self._check(self.lib.pcc_pack_fields(self.ctx, ntau, _p(a), _p(b), _p(c), _p(z)))
+        return z
+
+    def unpack(self, ntau, z):
+        """unpackSpectralFields(z) -> (U_p, psi_c, f_c)."""
+        z = _f64(z)
+        up, ps, fc = np.zeros(ntau), np.zeros(ntau), np.zeros(ntau)
+        self._check(self.lib.pcc_unpack_fields(self.ctx, ntau, _p(z), _p(up), _p(ps), _p(fc)))
+        return up, ps, fc
+
+    def expansions(self, ntau, dim, delta, xl, xr, fc, psic, up):
+        """(Y_left, Y_right) from time-domain fields."""
+        a, b, c = _f64(fc), _f64(psic), _f64(up)
+        yl, yr = np.zeros(ntau), np.zeros(ntau)
+        self._check(self.lib.pcc_expansions(self.ctx, ntau, dim, delta, xl, xr, _p(a), _p(b), _p(c), _p(yl),
+                                            _p(yr)))
+        return yl, yr
+
+    def dft(self, x, sign):
+        """Unscaled DFT exp(sign 2 pi i jk/n) of complex rows of x."""
+        x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.complex128)
+        out = np.zeros_like(x)
+        self._check(self.lib.pcc_dft(self.ctx, x.shape[1], x.shape[0], sign, x.ctypes.data_as(_D),
+                                     out.ctypes.data_as(_D)))
+        return out
+
     def fp64_peak_tflops(self):
         v = ctypes.c_double(0)
         self._check(self.lib.pcc_fp64_peak(self.ctx, ctypes.byref(v)))
@@ -200,15 +243,20 @@ class Solve:
         engine._check(self.lib.pcc_solve_create(engine.ctx, ctypes.byref(desc), ctypes.byref(self.h)))
 
     def close(self):
-        if self.h:
+        # a closed engine has already destroyed this solve with its context
+        if self.h and self.engine.ctx:
             self.lib.pcc_solve_destroy(self.h)
-            self.h = ctypes.c_void_p()
+        self.h = ctypes.c_void_p()
 
     def __del__(self):
         try:
             self.close()
         except Exception:
             pass
+
+    def set_grid(self, grid):
+        g = _f64(grid)
+        self.engine._check(self.lib.pcc_solve_set_grid(self.h, _p(g)))
 
     def grid(self):
         g = np.zeros(self.desc.nl + self.desc.nr + 1)

@@ -72,7 +72,7 @@ def perturb(z, rel, rng):
     return z * noise
 
 
-def case(R, cfg, in0, name, jac_cols, threads, full_newton=False):
+def case(R, cfg, in0, name, jac_idx, threads, full_newton=False):
     n, D = cfg["Ntau"], cfg["Dim"]
     nn = 3 * n // 4
     out = {"config": json.dumps({k: v for k, v in cfg.items() if k != "Initial_Conditions"}), "in0": in0}
@@ -100,13 +100,14 @@ def case(R, cfg, in0, name, jac_cols, threads, full_newton=False):
     out0 = R.shoot(cfg, in0)
     out["out0"] = out0
     out["t_shoot_s"] = time.time() - t
-    if jac_cols:
-        c0, c1 = jac_cols
+    if jac_idx is not None:
+        jac_idx = list(jac_idx)
         t = time.time()
-        out["jac_c0"] = c0
-        out["jac_cols"] = R.jacobian_columns(cfg, in0, out0, c0, c1, threads)
+        out["jac_idx"] = np.array(jac_idx)
+        out["jac_cols"] = np.concatenate([R.jacobian_columns(cfg, in0, out0, c, c + 1, 1) for c in jac_idx], axis=1) \
+            if len(jac_idx) < 16 else R.jacobian_columns(cfg, in0, out0, jac_idx[0], jac_idx[-1] + 1, threads)
         out["t_jac_s"] = time.time() - t
-        if full_newton and c0 == 0 and c1 == nn:
+        if full_newton and jac_idx == list(range(nn)):
             J = out["jac_cols"]
             dx = R.solve(J, -out0)
             err = np.sqrt(np.mean(out0 ** 2))
@@ -116,6 +117,27 @@ def case(R, cfg, in0, name, jac_cols, threads, full_newton=False):
                        newton_out1=R.shoot(cfg, in1))
     np.savez_compressed(HERE / f"ref_{name}.npz", **out)
     print(name, {k: (v.shape if hasattr(v, "shape") else v) for k, v in out.items() if k != "config"})
+
+
+def newton_to_convergence(R, cfg, in0, name, threads, iters=8):
+    """The reference's Newton loop (NewtonSolver.cpp:279-366) run from in0:
+    the converged solution and the residual history."""
+    nn = in0.size
+    x = in0.copy()
+    hist = []
+    for _ in range(iters):
+        out = R.shoot(cfg, x)
+        err = float(np.sqrt(np.mean(out ** 2)))
+        hist.append([err, x[2 * nn // 3 + 2]])
+        J = R.jacobian_columns(cfg, x, out, 0, nn, threads)
+        dx = R.solve(J, -out)
+        x = x + min(1.0, cfg["SlowError"] / err) * dx
+    out = R.shoot(cfg, x)
+    hist.append([float(np.sqrt(np.mean(out ** 2))), x[2 * nn // 3 + 2]])
+    np.savez_compressed(HERE / f"ref_{name}.npz", config=json.dumps({k: v for k, v in cfg.items()
+                                                                        if k != "Initial_Conditions"}),
+                        in0=in0, x_star=x, history=np.array(hist))
+    print(name, "history", hist)
 
 
 def main():
@@ -133,14 +155,16 @@ def main():
     # C1: Ntau=128, 1000+1000 points, full Jacobian and Newton step, fixture and seeded perturbation
     cfg = config(ref, 128, 1000, 1000)
     z = packed_input(R, cfg)
-    case(R, cfg, z, "c1_fixture", (0, 96), a.threads, full_newton=True)
-    case(R, cfg, perturb(z, 1e-3, rng), "c1_perturbed", (0, 96), a.threads, full_newton=True)
-    # C2: Ntau=512, 3000+3000: base shoot and a few columns
+    case(R, cfg, z, "c1_fixture", range(96), a.threads, full_newton=True)
+    zp = perturb(z, 1e-3, rng)
+    case(R, cfg, zp, "c1_perturbed", range(96), a.threads, full_newton=True)
+    newton_to_convergence(R, cfg, zp, "c1_newton", a.threads)
+    # C2: Ntau=512, 3000+3000: base shoot and the leading column of each field plus Delta
     cfg = config(ref, 512, 3000, 3000)
-    case(R, cfg, packed_input(R, cfg), "c2_fixture", (0, 4), a.threads)
-    # C3: Ntau=1024, 4000+4000: base shoot and a few columns
+    case(R, cfg, packed_input(R, cfg), "c2_fixture", [0, 128, 256, 258], a.threads)
+    # C3: Ntau=1024, 4000+4000: the same columns (Up mode 1, psi_c mode 1, f_c DC, Delta)
     cfg = config(ref, 1024, 4000, 4000)
-    case(R, cfg, packed_input(R, cfg), "c3_fixture", (510, 514), a.threads)
+    case(R, cfg, packed_input(R, cfg), "c3_fixture", [0, 256, 512, 514], a.threads)
 
 
 if __name__ == "__main__":

@@ -108,9 +108,9 @@ def test_shoot_and_columns_vs_reference(oracle):
     assert np.max(np.abs(out0 - d["out0"])) < 1e-10
     cols, st, _ = oracle.jacobian_columns(d["cfg"], d["in0"], d["out0"], 0, 2)
     assert st == 0
-    for k in range(2):
-        # eps = 1e-7 amplifies those differences to ~1e-5 relative
-        assert rel_err(cols[:, k], d["jac_cols"][:, k]) < 1e-3
+    # eps = 1e-7 amplifies those differences to ~1e-6 of max|J|
+    scale = np.max(np.abs(d["jac_cols"]))
+    assert np.max(np.abs(cols - d["jac_cols"][:, :2])) / scale < 2e-5
 
 
 def test_newton_update_reference_consistent(oracle):
