@@ -213,6 +213,16 @@ def run_engine(args, world, rank, local):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
     torch.cuda.synchronize()
 
+    if args.columns:
+        # a profiling case: columns [0, C) through the host ABI, one march launch per step
+        for _ in range(args.warmup + args.steps):
+            st = {}
+            solve.jacobian_columns(in0, out0, 0, args.columns, stats=st)
+            print(json.dumps({"profile_case": True, "columns": args.columns, **st}))
+        solve.close()
+        eng.close()
+        return
+
     for _ in range(args.warmup):
         solve.jacobian_device(d_in0.data_ptr(), d_out0.data_ptr(), d_J.data_ptr())
         solve.sync()
@@ -306,6 +316,8 @@ def main():
     ap.add_argument("--seed", type=int, default=1024)
     ap.add_argument("--amp", type=float, default=0.1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--columns", type=int, default=0,
+                    help="profiling aid: build only the first C columns (not a benchmark line)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args)
     try:

@@ -314,10 +314,11 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
     for (int q = 0; q < 8; ++q) F[q] = v[q].y;
 
     // --- IA2 constraint coefficients (InitialConditionGenerator.cpp:876-881) --
+    const double c8 = dm2c / (8.0 * x);  // (D-2)^3 / (8x), once per evaluation
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         const double U = Us[q * TG + t], V = Vs[q * TG + t];
-        const double co = -(((x + F[q]) * U * U + (x - F[q]) * V * V) * dm2c / (8.0 * x) + (dim - 3.0));
+        const double co = -(((x + F[q]) * U * U + (x - F[q]) * V * V) * c8 + (dim - 3.0));
         v[q] = make_double2(co, 0.0);
     }
 
@@ -326,7 +327,7 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = make_double2(v[q].x * invM, v[q].y * invM);
     if (active && t == 0) *lam_slot = v[0].x;  // lambda = f_hat[0] (real: imag is exactly 0)
-    // lamIntegrate(f_hat, 0): out_k = f_k / (0 - i m k0), DC and Nyquist -> 0
+    // lamIntegrate(f_hat, 0): out_k = f_k / (-i m k0) = i f_k / (m k0); DC and Nyquist -> 0
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         const int p = t + TG * q;
@@ -335,41 +336,47 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
             v[q] = make_double2(0.0, 0.0);
         } else {
             const int m = k < M ? k : k - N;
-            v[q] = cdiv(v[q].x, v[q].y, 0.0, 0.0 - m * k0);
+            const double r = 1.0 / (m * k0);
+            v[q] = make_double2(-v[q].y * r, v[q].x * r);
         }
     }
     dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
     double Fr[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        Fr[q] = v[q].x;
-        v[q] = make_double2(-(dim - 3.0) * exp(Fr[q]), 0.0);  // h = -g e^F
+        const double e = exp(v[q].x);
+        Fr[q] = 1.0 / e;                         // e^{-F}, kept for X e^{-F}
+        v[q] = make_double2(-(dim - 3.0) * e, 0.0);  // h = -g e^F
     }
     dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
     const double lam = *lam_slot;  // written before at least one sweep barrier
     {
         const double s = k0 * N / 2.0;
         const double2 qn = cdiv(lam, 0.0, lam * lam - 0.0 * 0.0 + s * s, lam * 0.0 + 0.0 * lam);
+        // out_k = h_k / (lambda - i s) = h_k (lambda + i s) / (lambda^2 + s^2), s = m k0
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int p = t + TG * q;
             const int k = 2 * p;
             const double2 h = make_double2(v[q].x * invM, v[q].y * invM);
             if (p == 0) {
-                v[q] = lam != 0.0 ? cdiv(h.x, h.y, lam, 0.0) : make_double2(0.0, 0.0);
+                v[q] = lam != 0.0 ? make_double2(h.x / lam, h.y / lam) : make_double2(0.0, 0.0);
             } else if (k == M) {
                 v[q] = cmul(qn, h);
             } else {
                 const int m = k < M ? k : k - N;
-                const double dr = lam - 0.0, di = 0.0 - m * k0;
-                v[q] = (hypot(dr, di) < 1e-14) ? make_double2(0.0, 0.0) : cdiv(h.x, h.y, dr, di);
+                const double sm = m * k0;
+                const double den = lam * lam + sm * sm;  // |lambda - i s|^2
+                const double r = 1.0 / den;
+                v[q] = den < 1e-28 ? make_double2(0.0, 0.0)
+                                   : make_double2((h.x * lam - h.y * sm) * r, (h.y * lam + h.x * sm) * r);
             }
         }
     }
     dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
     double IA2[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) IA2[q] = v[q].x * exp(-Fr[q]);
+    for (int q = 0; q < 8; ++q) IA2[q] = v[q].x * Fr[q];  // X e^{-F}
 
     // --- dU + i dV from -i m k0 c on the odd modes ---------------------------
 #pragma unroll
@@ -388,6 +395,9 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
     dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
 
     // --- pointwise Einstein-scalar RHS (ODEStepper.cpp:109-122) ---------------
+    // divisions are taken as reciprocals shared between terms (one for 1/IA2,
+    // one for both characteristic denominators): ulp-level rounding changes
+    const double xinv = 1.0 / x;
     double fx[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -396,11 +406,13 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
         const double2 dO = cmul(v[q], cconj(w));
         const double dU = dO.x, dV = dO.y;
         const double U = Us[q * TG + t], V = Vs[q * TG + t];
-        const double ux = (F[q] * ((dim - 2.0) * V - (2.0 * (dim - 3.0) / IA2[q] - (dim - 2.0)) * U) - 2.0 * x * dU) /
-                          (2.0 * x * (F[q] + x));
-        const double vx = (F[q] * ((dim - 2.0) * U - (2.0 * (dim - 3.0) / IA2[q] - (dim - 2.0)) * V) + 2.0 * x * dV) /
-                          (2.0 * x * (F[q] - x));
-        fx[q] = (dim - 3.0) * F[q] * (1.0 - IA2[q]) / (IA2[q] * x);
+        const double ia = 1.0 / IA2[q];
+        const double g = 2.0 * (dim - 3.0) * ia - (dim - 2.0);
+        const double fp = 2.0 * x * (F[q] + x), fm = 2.0 * x * (F[q] - x);
+        const double rr = 1.0 / (fp * fm);  // one reciprocal for both denominators
+        const double ux = (F[q] * ((dim - 2.0) * V - g * U) - 2.0 * x * dU) * (fm * rr);
+        const double vx = (F[q] * ((dim - 2.0) * U - g * V) + 2.0 * x * dV) * (fp * rr);
+        fx[q] = (dim - 3.0) * F[q] * (1.0 - IA2[q]) * ia * xinv;
         v[q] = cmul(make_double2(ux, vx), w);  // pre-twiddle exp(+2 pi i j/N)
     }
 
