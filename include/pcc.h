@@ -166,6 +166,23 @@ pcc_status pcc_sweep(pcc_solve* s, int count, const int* sides, const double* y_
 pcc_status pcc_expansions(pcc_ctx* ctx, int ntau, double dim, double delta, double x_l, double x_r,
                           const double* fc, const double* psic, const double* up, double* y_left, double* y_right);
 
+/* Allocation-free variant of pcc_expansions; it has no counterpart in the
+ * reference.  For callers that may not allocate device memory once they are
+ * running (a service that reserves its whole device-memory pool at start-up,
+ * a library that must not trigger the device synchronisation cudaFree can
+ * cause): the caller passes device pointers for the inputs (fc, psic, up:
+ * Ntau doubles each) and outputs (y_left, y_right: Ntau doubles each; NULL
+ * skips a side), and the work arrays live in a static device array compiled
+ * into the library (1.3 MiB, kept by every GPU that loads the library until
+ * the process exits), so Ntau is limited to 2048; larger values are rejected
+ * with PCC_ERR_INVALID_ARG.  The call is asynchronous on the context stream
+ * and allocates nothing.  Its first call on a device looks up the array's
+ * device address; make that first call before any stream capture.  All calls
+ * share the one array, so calls that overlap on the GPU race. */
+pcc_status pcc_expansions_static(pcc_ctx* ctx, int ntau, double dim, double delta, double x_l, double x_r,
+                                 const double* d_fc, const double* d_psic, const double* d_up, double* d_y_left,
+                                 double* d_y_right);
+
 /* Replaces the solve's x-grid (NewtonSolver::generateGrid output) by grid,
  * NLeft + NRight + 1 points, as ShootingSolver::shoot accepts any gridX. */
 pcc_status pcc_solve_set_grid(pcc_solve* s, const double* grid);

@@ -65,6 +65,10 @@ struct pcc_solve {
     MarchLaunchInfo last_launch{};
 };
 
+cudaStream_t pcc_ctx_stream(pcc_ctx* ctx) { return ctx->stream; }
+int pcc_ctx_device(pcc_ctx* ctx) { return ctx->device; }
+void pcc_ctx_set_error(pcc_ctx* ctx, const char* msg) { ctx->last_error = msg; }
+
 namespace {
 
 const char* kStatusNames[] = {"PCC_OK",

@@ -44,3 +44,9 @@ size_t lu_mixed_work_bytes(int n);
 cudaError_t fp64_peak_probe(double* tflops, cudaStream_t st);
 
 }  // namespace pcc
+
+// accessors of the opaque context (pcc_abi.cu)
+struct pcc_ctx;
+cudaStream_t pcc_ctx_stream(pcc_ctx* ctx);
+int pcc_ctx_device(pcc_ctx* ctx);
+void pcc_ctx_set_error(pcc_ctx* ctx, const char* msg);

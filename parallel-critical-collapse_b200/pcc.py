@@ -34,7 +34,7 @@ EXPORTS = ["pcc_ctx_create", "pcc_ctx_destroy", "pcc_status_string", "pcc_last_e
            "pcc_solve_destroy", "pcc_solve_grid", "pcc_shoot", "pcc_jacobian", "pcc_jacobian_device",
            "pcc_solve_sync", "pcc_jacobian_columns", "pcc_lu_solve", "pcc_newton_step", "pcc_rhs_eval",
            "pcc_irk_step", "pcc_boundary_data", "pcc_sweep", "pcc_fp64_peak", "pcc_pack_fields",
-           "pcc_unpack_fields", "pcc_expansions", "pcc_solve_set_grid", "pcc_dft"]
+           "pcc_unpack_fields", "pcc_expansions", "pcc_solve_set_grid", "pcc_dft", "pcc_expansions_static"]
 
 
 class PccError(RuntimeError):
@@ -119,6 +119,7 @@ def load(path=None):
     L.pcc_expansions.argtypes = [vp, ci, cd, cd, cd, cd, _D, _D, _D, _D, _D]
     L.pcc_solve_set_grid.argtypes = [vp, _D]
     L.pcc_dft.argtypes = [vp, ci, ci, ci, _D, _D]
+    L.pcc_expansions_static.argtypes = [vp, ci, cd, cd, cd, cd, vp, vp, vp, vp, vp]
     for name in EXPORTS:
         if name not in ("pcc_status_string", "pcc_last_error"):
             getattr(L, name).restype = ci
