@@ -143,11 +143,32 @@ __device__ __forceinline__ void dft8(double2 (&a)[8])
     a[6] = t;
 }
 
+// Twiddles of one Stockham pass (radix R, span NS) for thread t: element r of
+// butterfly u = t + TG u' is multiplied by w_M^{SG r k M/(NS R)}, k = j mod NS.
+// Fetched separately so that the loads can be issued before the barrier that
+// precedes the pass and their latency overlaps the barrier wait.
+template <int M, int TG, int R, int NS, int SG>
+__device__ __forceinline__ void fetch_twiddles(double2 (&w)[7], int t, const double2* __restrict__ twN, int zoff)
+{
+    constexpr int B = 8 / R;
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+        const int k = (t + TG * u) & (NS - 1);
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+            const int idx = r * k * (M / (NS * R));  // exponent of w_M, < M
+            double2 x = __ldg(&twN[2 * idx + zoff]);
+            if (SG < 0) x.y = -x.y;
+            w[u * (R - 1) + (r - 1)] = x;
+        }
+    }
+}
+
 // One Stockham pass of radix R over span NS on the standard layout: thread t
 // holds x[t + TG q]; butterfly j = t + TG u takes x[j + r M/R] = v[u + r*8/R].
 template <int M, int TG, int R, int NS, int SG, bool LAST>
 __device__ __forceinline__ void stockham_pass(double2 (&v)[8], double2* __restrict__ out, int t,
-                                              const double2* __restrict__ twN, int zoff)
+                                              const double2 (&w)[7])
 {
     constexpr int B = 8 / R;
 #pragma unroll
@@ -159,12 +180,7 @@ __device__ __forceinline__ void stockham_pass(double2 (&v)[8], double2* __restri
         for (int r = 0; r < R; ++r) a[r] = v[u + r * B];
         if (NS > 1) {
 #pragma unroll
-            for (int r = 1; r < R; ++r) {
-                const int idx = r * k * (M / (NS * R));  // exponent of w_M, < M
-                double2 w = __ldg(&twN[2 * idx + zoff]);
-                if (SG < 0) w.y = -w.y;
-                a[r] = cmul(a[r], w);
-            }
+            for (int r = 1; r < R; ++r) a[r] = cmul(a[r], w[u * (R - 1) + (r - 1)]);
         }
         if (R == 8) {
             dft8<SG>(a);
@@ -185,6 +201,13 @@ __device__ __forceinline__ void stockham_pass(double2 (&v)[8], double2* __restri
 }
 
 template <int TG>
+__device__ __forceinline__ void fetch_point_twiddles(double2* pj, int t, const double2* __restrict__ twN, int zoff)
+{
+#pragma unroll
+    for (int q = 0; q < 8; ++q) pj[q] = __ldg(&twN[t + TG * q + zoff]);
+}
+
+template <int TG>
 __device__ __forceinline__ void load_std(double2 (&v)[8], const double2* __restrict__ in, int t)
 {
 #pragma unroll
@@ -195,40 +218,55 @@ __device__ __forceinline__ void load_std(double2 (&v)[8], const double2* __restr
 // standard register layout.  bufs[0..1] ping-pong; `cur` selects the first
 // buffer written and is advanced so that the next transform never writes a
 // buffer that a lagging thread may still be reading.
+// pj (optional): the per-point twiddles w_N^{t + TG q}, q < 8, fetched before
+// the transform's last barrier for the caller's post-twiddle.
 template <int M, int TG, int SG>
 __device__ __forceinline__ void dft_m(double2 (&v)[8], double2* __restrict__ b0, double2* __restrict__ b1,
                                       int& cur, int t, const double2* __restrict__ twN, const SweepSync& sy,
-                                      bool active, const volatile int* zero)
+                                      bool active, const volatile int* zero, double2* pj = nullptr)
 {
     constexpr int NP = M == 64 ? 2 : (M <= 512 ? 3 : 4);
     constexpr int RL = M == 64 ? 8 : M == 128 ? 2 : M == 256 ? 4 : M == 512 ? 8 : 2;
+    // A zero read from shared memory, added to every twiddle index of this
+    // transform: the backend cannot prove two transforms use the same twiddle
+    // addresses, so it does not keep all of them live in registers across the
+    // whole RHS evaluation (which costs ~50 registers and spills).
+    const int zoff = *zero;
     double2* w0 = cur ? b1 : b0;
     double2* w1 = cur ? b0 : b1;
-    if (active) stockham_pass<M, TG, 8, 1, SG, false>(v, w0, t, twN, 0);
-    sy.sync();
-    if (active) load_std<TG>(v, w0, t);
-    // A zero read from shared memory after the barrier, added to every twiddle
-    // index of this transform: the backend cannot prove two transforms use the
-    // same twiddle addresses, so it does not keep all of them live in
-    // registers across the whole RHS evaluation (which costs ~50 registers and
-    // spills).  `zero` is the sweep's constant-zero word.
-    const int zoff = *zero;
+    double2 tw[7];
+    if (active) stockham_pass<M, TG, 8, 1, SG, false>(v, w0, t, tw);  // span 1: no twiddles
     if constexpr (NP == 2) {
-        if (active) stockham_pass<M, TG, RL, 8, SG, true>(v, w0, t, twN, zoff);
-        cur ^= 1;
-    } else if constexpr (NP == 3) {
-        if (active) stockham_pass<M, TG, 8, 8, SG, false>(v, w1, t, twN, zoff);
-        sy.sync();
-        if (active) load_std<TG>(v, w1, t);
-        if (active) stockham_pass<M, TG, RL, 64, SG, true>(v, w1, t, twN, zoff);
-    } else {
-        if (active) stockham_pass<M, TG, 8, 8, SG, false>(v, w1, t, twN, zoff);
-        sy.sync();
-        if (active) load_std<TG>(v, w1, t);
-        if (active) stockham_pass<M, TG, 8, 64, SG, false>(v, w0, t, twN, zoff);
+        if (active) fetch_twiddles<M, TG, RL, 8, SG>(tw, t, twN, zoff);
+        if (pj && active) fetch_point_twiddles<TG>(pj, t, twN, zoff);
         sy.sync();
         if (active) load_std<TG>(v, w0, t);
-        if (active) stockham_pass<M, TG, RL, 512, SG, true>(v, w0, t, twN, zoff);
+        if (active) stockham_pass<M, TG, RL, 8, SG, true>(v, w0, t, tw);
+        cur ^= 1;
+    } else if constexpr (NP == 3) {
+        if (active) fetch_twiddles<M, TG, 8, 8, SG>(tw, t, twN, zoff);
+        sy.sync();
+        if (active) load_std<TG>(v, w0, t);
+        if (active) stockham_pass<M, TG, 8, 8, SG, false>(v, w1, t, tw);
+        if (active) fetch_twiddles<M, TG, RL, 64, SG>(tw, t, twN, zoff);
+        if (pj && active) fetch_point_twiddles<TG>(pj, t, twN, zoff);
+        sy.sync();
+        if (active) load_std<TG>(v, w1, t);
+        if (active) stockham_pass<M, TG, RL, 64, SG, true>(v, w1, t, tw);
+    } else {
+        if (active) fetch_twiddles<M, TG, 8, 8, SG>(tw, t, twN, zoff);
+        sy.sync();
+        if (active) load_std<TG>(v, w0, t);
+        if (active) stockham_pass<M, TG, 8, 8, SG, false>(v, w1, t, tw);
+        if (active) fetch_twiddles<M, TG, 8, 64, SG>(tw, t, twN, zoff);
+        sy.sync();
+        if (active) load_std<TG>(v, w1, t);
+        if (active) stockham_pass<M, TG, 8, 64, SG, false>(v, w0, t, tw);
+        if (active) fetch_twiddles<M, TG, RL, 512, SG>(tw, t, twN, zoff);
+        if (pj && active) fetch_point_twiddles<TG>(pj, t, twN, zoff);
+        sy.sync();
+        if (active) load_std<TG>(v, w0, t);
+        if (active) stockham_pass<M, TG, RL, 512, SG, true>(v, w0, t, tw);
         cur ^= 1;
     }
 }
@@ -286,11 +324,11 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
         v[6] = yks[4 * TG + t];
         v[7] = yks[6 * TG + t];
     }
-    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
+    double2 pj[8];
+    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero, pj);
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const int j = t + TG * q;
-        const double2 o = cmul(v[q], cconj(__ldg(&twN[j])));
+        const double2 o = cmul(v[q], cconj(pj[q]));
         if (active) {
             Us[q * TG + t] = o.x;
             Vs[q * TG + t] = o.y;
@@ -392,7 +430,7 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
             v[q] = make_double2(s * a.y, -(s * a.x));
         }
     }
-    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
+    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero, pj);
 
     // --- pointwise Einstein-scalar RHS (ODEStepper.cpp:109-122) ---------------
     // divisions are taken as reciprocals shared between terms (one for 1/IA2,
@@ -401,8 +439,7 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
     double fx[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const int j = t + TG * q;
-        const double2 w = __ldg(&twN[j]);
+        const double2 w = pj[q];
         const double2 dO = cmul(v[q], cconj(w));
         const double dU = dO.x, dV = dO.y;
         const double U = Us[q * TG + t], V = Vs[q * TG + t];
