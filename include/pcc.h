@@ -136,6 +136,60 @@ pcc_status pcc_lu_solve(pcc_ctx* ctx, int n, const double* A, const double* rhs,
 pcc_status pcc_newton_step(pcc_solve* s, double* in0, double* err_out, pcc_precision prec, pcc_stats* stats,
                            pcc_refine_report* report);
 
+/* ---- batches of solves and the device-resident Newton loop --------------
+ * Several solves of one context (different Dim, Ntau and grid sizes) share
+ * ONE persistent march launch: every sweep of every listed solve is an item
+ * of that launch.  Solves with Ntau 128..1024 and 2 IRK stages batch; others
+ * run their own launch inside the same call.  The result of a solve does not
+ * depend on what it is batched with: each sweep is computed by one sweep slot
+ * with the same arithmetic. */
+
+/* assembleJacobian for count solves at once (host arrays, J[i] row-major
+ * Nnewton_i x Nnewton_i).  Every solve must batch (PCC_ERR_UNSUPPORTED). */
+pcc_status pcc_jacobian_batch(pcc_ctx* ctx, int count, pcc_solve* const* solves, const double* const* in0,
+                              const double* const* out0, double* const* J, pcc_stats* stats);
+
+/* Newton state codes: how NewtonSolver::run (NewtonSolver.cpp:279-372) ends. */
+typedef enum {
+    PCC_NEWTON_RUNNING = 0,
+    PCC_NEWTON_CONVERGED = 1,      /* mismatch RMS < PrecisionNewton (:303-309) */
+    PCC_NEWTON_STOPPED = 2,        /* mismatch grew 5 times: result = last improving iterate (:312-325) */
+    PCC_NEWTON_MAX_ITER = 3,       /* MaxIterNewton iterations without convergence (:368-372) */
+    PCC_NEWTON_IRK_FAILED = 4,     /* a sweep's IRK iteration failed (ShootingSolver.cpp:69-82) */
+    PCC_NEWTON_DELTA_MISMATCH = 5, /* ShootingSolver.cpp:167-178 */
+    PCC_NEWTON_SINGULAR = 6        /* zero pivot (NewtonSolver.cpp:751-755) */
+} pcc_newton_code;
+
+typedef struct {
+    int iterations;          /* base shoots evaluated */
+    int code;                /* pcc_newton_code */
+    double err;              /* mismatch RMS of the last base shoot */
+    double err_old;          /* of the one before */
+    int fail_column, fail_side, fail_grid_index; /* IRK failure location, else -1 */
+    int lu_refinement_steps; /* last mixed-precision solve's refinement sweeps (-1: FP64 solve) */
+    int lu_fell_back;        /* last mixed-precision solve fell back to the FP64 factorisation */
+} pcc_newton_state;
+
+/* Starts NewtonSolver::run's loop on the device from in0 (host, Nnewton):
+ * err = errOld = 1, no increases, in0old = in0 (NewtonSolver.cpp:268-277). */
+pcc_status pcc_newton_begin(pcc_solve* s, const double* in0);
+
+/* One loop iteration for every listed solve still running: base shoot and
+ * all Jacobian columns of all of them in one batch launch, then per solve on
+ * the device the convergence test and divergence safeguard, J, the Newton
+ * solve (prec) and the damped update.  states[i] (optional) is solve i's
+ * state afterwards; stats (optional) describes the launch. */
+pcc_status pcc_newton_iterate(pcc_ctx* ctx, int count, pcc_solve* const* solves, pcc_precision prec,
+                              pcc_newton_state* states, pcc_stats* stats);
+
+/* The solve's result: the converged (or last) iterate, or for
+ * PCC_NEWTON_STOPPED the last improving one; Delta at in0_out[2N/3+2]. */
+pcc_status pcc_newton_result(pcc_solve* s, double* in0_out, pcc_newton_state* state);
+
+/* begin + iterate until no solve is running + result, in0[i] in place. */
+pcc_status pcc_newton_solve(pcc_ctx* ctx, int count, pcc_solve* const* solves, double* const* in0,
+                            pcc_precision prec, pcc_newton_state* states, pcc_stats* stats);
+
 /* ---- lower-level entry points (the reference's inner class methods) ---- */
 
 /* ODEStepper::computeDerivatives (ODEStepper.cpp:92-136) for `count` states:

@@ -68,6 +68,37 @@ cudaError_t PCC_CAT(launch_march_n, PCC_MARCH_N)(int stages, const MarchParams& 
 }
 #endif
 
+#ifdef PCC_MARCH_BATCH
+bool march_batch_supported(int ntau, int stages)
+{
+    return stages == 2 && (ntau == 128 || ntau == 256 || ntau == 512 || ntau == 1024);
+}
+
+cudaError_t launch_march_batch(const BatchParams& B, int max_ctas, cudaStream_t st, MarchLaunchInfo* info)
+{
+    using K = BatchShape<2>;
+    auto kern = march_batch_kernel<2>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, K::NT, K::SMEM)) != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    int ctas = sms * per_sm;
+    if (max_ctas > 0 && ctas > max_ctas) ctas = max_ctas;
+    if (info) {
+        info->ctas = ctas;
+        info->sweeps_per_cta = 0;  // depends on the class
+        info->threads = K::NT;
+        info->smem = K::SMEM;
+        info->ctas_per_sm = per_sm;
+    }
+    kern<<<ctas, K::NT, K::SMEM, st>>>(B);
+    return cudaGetLastError();
+}
+#endif
+
 #ifdef PCC_MARCH_DISPATCH
 cudaError_t launch_march_n128(int, const MarchParams&, int, cudaStream_t, MarchLaunchInfo*);
 cudaError_t launch_march_n256(int, const MarchParams&, int, cudaStream_t, MarchLaunchInfo*);

@@ -500,208 +500,442 @@ __device__ __forceinline__ double sweep_sum(double x, double* red, int lt, const
     }
 }
 
+// ------------------------------------------------------------ sweep slot
+// Shared-memory partition and thread roles of one sweep slot of a CTA.
+template <int N, int S>
+struct Slot {
+    using K = MarchShape<N, S>;
+    double2* ex;    // [S][2][MP]; the stage RHS lands in one buffer of each pair
+    double2* ys;    // [8][TG] slot-indexed y
+    double2* ykm;   // this group's stage values [8][TG]
+    double* uvm;    // this group's U, V [2][M]
+    double* lam;    // [S]
+    double* red;    // [NW]
+    int* item_slot;
+    volatile int* zero;
+    double2* b0;
+    double2* b1;
+    int slot_id, lt, s, t;
+    bool active;
+    SweepSync sy;
+
+    __device__ __forceinline__ Slot(double2* smem, int tid)
+    {
+        constexpr int TG = K::TG, STP = K::STP;
+        slot_id = tid / STP;
+        lt = tid % STP;
+        const int s_raw = lt / TG;
+        active = s_raw < S;
+        s = active ? s_raw : S - 1;
+        t = lt % TG;
+        if constexpr (STP < 32) {
+            sy.bar_id = 0;
+            sy.nthreads = STP;
+            sy.mask = ((1u << STP) - 1u) << ((tid & 31) / STP * STP);
+        } else if constexpr (STP == 32) {
+            sy.bar_id = 0;
+            sy.nthreads = 32;
+            sy.mask = 0xffffffffu;
+        } else {
+            sy.bar_id = 1 + slot_id;
+            sy.nthreads = STP;
+            sy.mask = 0xffffffffu;
+        }
+        double2* base = smem + (size_t)slot_id * K::PER_SWEEP;
+        ex = base;
+        ys = ex + K::EX;
+        double2* yks = ys + K::YS;
+        double* uv = reinterpret_cast<double*>(yks + K::YK);
+        double* misc = uv + 2 * K::UV;
+        lam = misc;
+        red = misc + S;
+        item_slot = reinterpret_cast<int*>(misc + S + K::NW);
+        zero = item_slot + 1;
+        b0 = ex + (size_t)s * 2 * K::MP;
+        b1 = b0 + K::MP;
+        ykm = yks + (size_t)s * 8 * TG;
+        uvm = uv + (size_t)s * 2 * K::M;
+    }
+};
+
+// state -> slots: y (group 0) and every stage value (its own group)
+template <int N, int S>
+__device__ __forceinline__ void load_state(const Slot<N, S>& sl, const double* __restrict__ yin)
+{
+    constexpr int TG = MarchShape<N, S>::TG;
+    if (sl.active) {
+#pragma unroll
+        for (int sg = 0; sg < 8; ++sg) {
+            const int m = slot_mode<N>(sg, sl.t);
+            const double2 v = make_double2(yin[2 * m], yin[2 * m + 1]);
+            sl.ykm[sg * TG + sl.t] = v;
+            if (sl.s == 0) sl.ys[sg * TG + sl.t] = v;
+        }
+    }
+}
+
+// Per-sweep values of the single-solve kernel: kernel parameters.
+struct ParamScalars {
+    const MarchParams& P;
+    __device__ __forceinline__ double dim() const { return P.dim; }
+    __device__ __forceinline__ double dm2c() const { return P.dim_m2_cubed; }
+    __device__ __forceinline__ double prec() const { return P.prec; }
+    __device__ __forceinline__ int max_its() const { return P.max_its; }
+    __device__ __forceinline__ int nl() const { return P.nl; }
+    __device__ __forceinline__ int nr() const { return P.nr; }
+    __device__ __forceinline__ double grid(int i) const { return P.grid[i]; }
+    __device__ __forceinline__ const double2* twN() const { return P.twN; }
+    __device__ __forceinline__ double a(int i, int j) const { return P.a[i][j]; }
+    __device__ __forceinline__ double b(int i) const { return P.b[i]; }
+    __device__ __forceinline__ double c(int i) const { return P.c[i]; }
+    __device__ __forceinline__ int mode() const { return P.mode; }
+    __device__ __forceinline__ double x_in(int item) const { return P.x_in[item]; }
+    __device__ __forceinline__ double x_out(int item) const { return P.x_out[item]; }
+    __device__ __forceinline__ double* yout(int item, int n) const { return P.yfinal + (size_t)item * n; }
+    __device__ __forceinline__ int* status(int item) const { return P.status + item; }
+    __device__ __forceinline__ int* fail_index(int item) const { return P.fail_index + item; }
+    __device__ __forceinline__ int* its_out(int item) const { return P.its_out ? P.its_out + item : nullptr; }
+};
+
+// ------------------------------------------------------------ one sweep
+// March one (column, side) sweep: ShootingSolver::integrateToMatchPoint's
+// loop over the grid (ShootingSolver.cpp:53-145) with ODEStepper::stepIRK's
+// fixed-point iteration (ODEStepper.cpp:163-292) at every step.  Mode 2
+// takes the single step x_in -> x_out instead (the IRK step test entry).
+// The caller has loaded the state (load_state) and synchronised.  Outputs
+// are addressed through sc only where they are written, so that no output
+// pointer stays live across the march.
+template <int N, int S, class SC>
+__device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S>& sl, double k0, int side, int item,
+                                           unsigned long long& n_its, unsigned long long& n_steps)
+{
+    const int mode = sc.mode();
+    using K = MarchShape<N, S>;
+    constexpr int TG = K::TG, STP = K::STP;
+    const int s = sl.s, t = sl.t;
+    const bool active = sl.active;
+    double2* const ex = sl.ex;
+    double2* const ys = sl.ys;
+    double2* const ykm = sl.ykm;
+    int cur = 0;
+    const int nsteps = mode == 2 ? 1 : (side == 0 ? sc.nl() : sc.nr());
+    int status = 0, fail_at = -1;
+
+    for (int st = 0; st < nsteps; ++st) {
+        double xin, xout;
+        int gi;
+        if (mode == 2) {
+            xin = sc.x_in(item);
+            xout = sc.x_out(item);
+            gi = 0;
+        } else if (side == 0) {
+            gi = st;
+            xin = sc.grid(gi);
+            xout = sc.grid(gi + 1);
+        } else {
+            gi = sc.nl() + sc.nr() - st;
+            xin = sc.grid(gi);
+            xout = sc.grid(gi - 1);
+        }
+        const double dx = xout - xin;
+        const double xs = xin + dx * sc.c(s);
+
+        bool converged = false;
+        int its_reached = 0;
+        const int max_its = sc.max_its();
+        for (int its = 0; its < max_its; ++its) {
+            ++its_reached;
+            rhs_eval<N>(ykm, sl.uvm, xs, sc.dim(), sc.dm2c(), k0, t, sl.b0, sl.b1, cur, &sl.lam[s], sc.twN(), sl.sy,
+                        active, sl.zero);
+            sl.sy.sync();  // every stage RHS is in shared memory
+            double part = 0.0;
+            if (active) {
+#pragma unroll
+                for (int sg = 0; sg < 8; ++sg) {
+                    double2 nv = ys[sg * TG + t];
+#pragma unroll
+                    for (int kk = 0; kk < S; ++kk) {
+                        const double w = dx * sc.a(s, kk);
+                        const double2 f = ex[(size_t)(kk * 2 + cur) * K::MP + sg * TG + t];
+                        nv.x = fma(w, f.x, nv.x);
+                        nv.y = fma(w, f.y, nv.y);
+                    }
+                    const double2 old = ykm[sg * TG + t];
+                    const double ex_ = old.x - nv.x, ey_ = old.y - nv.y;
+                    part = fma(ex_, ex_, part);
+                    part = fma(ey_, ey_, part);
+                    ykm[sg * TG + t] = nv;
+                }
+            }
+            const double tot = sweep_sum<STP, K::NW>(part, sl.red, sl.lt, sl.sy);
+            const double norm2 = sqrt(tot / (double)(N * S));
+            const double prec = sc.prec();
+            double p10 = prec;
+            if (its > max_its / 2) p10 = prec * 10.0 * (2.0 * (double)its / (double)max_its - 0.5);
+            if (norm2 < p10) {
+                converged = true;
+                break;
+            }
+            if constexpr (K::NW == 1) sl.sy.sync();  // new stage values visible to every lane
+        }
+        n_its += its_reached;
+        n_steps += 1;
+        // y += dx sum_i b_i f_i with the RHS of the last evaluation; stages restart at y
+        if (active) {
+#pragma unroll
+            for (int sg = 0; sg < 8; ++sg) {
+                double2 y = ys[sg * TG + t];
+#pragma unroll
+                for (int i = 0; i < S; ++i) {
+                    const double w = dx * sc.b(i);
+                    const double2 f = ex[(size_t)(i * 2 + cur) * K::MP + sg * TG + t];
+                    y.x = fma(w, f.x, y.x);
+                    y.y = fma(w, f.y, y.y);
+                }
+                ykm[sg * TG + t] = y;
+            }
+        }
+        sl.sy.sync();  // every group has read the old y
+        if (active && s == 0) {
+#pragma unroll
+            for (int sg = 0; sg < 8; ++sg) ys[sg * TG + t] = ykm[sg * TG + t];
+        }
+        if (mode == 2 && active && s == 0 && t == 0) {
+            int* its_out = sc.its_out(item);
+            if (its_out) *its_out = converged ? its_reached : -its_reached;
+        }
+        if (!converged) {
+            status = 1;
+            fail_at = gi;
+            break;
+        }
+    }
+    // write the final state
+    if (active && s == 0) {
+        double* yout = sc.yout(item, N);
+#pragma unroll
+        for (int sg = 0; sg < 8; ++sg) {
+            const int m = slot_mode<N>(sg, t);
+            const double2 y = ys[sg * TG + t];
+            yout[2 * m] = y.x;
+            yout[2 * m + 1] = y.y;
+        }
+        if (t == 0) {
+            *sc.status(item) = status;
+            *sc.fail_index(item) = fail_at;
+        }
+    }
+    sl.sy.sync();
+}
+
 // ------------------------------------------------------------------ kernel
 template <int N, int S, int MINB>
 __global__ void __launch_bounds__(MarchShape<N, S>::NT, MINB) march_kernel(MarchParams P)
 {
     using K = MarchShape<N, S>;
-    constexpr int TG = K::TG, STP = K::STP;
+    constexpr int TG = K::TG;
     extern __shared__ double2 smem[];
-
-    const int slot_id = threadIdx.x / STP;
-    const int lt = threadIdx.x % STP;
-    const int s_raw = lt / TG;
-    const bool active = s_raw < S;
-    const int s = active ? s_raw : S - 1;
-    const int t = lt % TG;
-
-    SweepSync sy;
-    if constexpr (STP < 32) {
-        sy.bar_id = 0;
-        sy.nthreads = STP;
-        sy.mask = ((1u << STP) - 1u) << ((threadIdx.x & 31) / STP * STP);
-    } else if constexpr (STP == 32) {
-        sy.bar_id = 0;
-        sy.nthreads = 32;
-        sy.mask = 0xffffffffu;
-    } else {
-        sy.bar_id = 1 + slot_id;
-        sy.nthreads = STP;
-        sy.mask = 0xffffffffu;
-    }
-
-    double2* base = smem + (size_t)slot_id * K::PER_SWEEP;
-    double2* ex = base;            // [S][2][MP]; stage RHS lands in one of each pair
-    double2* ys = ex + K::EX;      // [8][TG]
-    double2* yks = ys + K::YS;     // [S][8][TG]
-    double* uv = reinterpret_cast<double*>(yks + K::YK);  // [S][2][M]
-    double* misc = uv + 2 * K::UV;
-    double* lam = misc;            // [S]
-    double* red = misc + S;        // [NW]
-    int* item_slot = reinterpret_cast<int*>(misc + S + K::NW);
-    volatile int* zero_slot = item_slot + 1;
-    if (lt == 0) *zero_slot = 0;
-
-    double2* b0 = ex + (size_t)s * 2 * K::MP;
-    double2* b1 = b0 + K::MP;
-    double2* ykm = yks + (size_t)s * 8 * TG;
-    double* uvm = uv + (size_t)s * 2 * K::M;
-
-    const double dim = P.dim;
+    const Slot<N, S> sl(smem, threadIdx.x);
+    if (sl.lt == 0) *sl.zero = 0;
+    const ParamScalars sc{P};
     unsigned long long n_its = 0, n_steps = 0;
 
     for (;;) {
-        if (lt == 0) *item_slot = atomicAdd(P.work_counter, 1);
-        sy.sync();
-        const int item = *item_slot;
-        sy.sync();
+        if (sl.lt == 0) *sl.item_slot = atomicAdd(P.work_counter, 1);
+        sl.sy.sync();
+        const int item = *sl.item_slot;
+        sl.sy.sync();
         if (item >= P.n_items) break;
 
         const double* yin = P.yinit + (size_t)item * N;
         const double delta = yin[4];
         const double k0 = 2.0 * kPi / delta;
-
-        // state -> slots: y (group 0) and every stage value (its own group)
-        if (active) {
-#pragma unroll
-            for (int sg = 0; sg < 8; ++sg) {
-                const int m = slot_mode<N>(sg, t);
-                const double2 v = make_double2(yin[2 * m], yin[2 * m + 1]);
-                ykm[sg * TG + t] = v;
-                if (s == 0) ys[sg * TG + t] = v;
-            }
-        }
-        int cur = 0;
-        sy.sync();
+        load_state<N, S>(sl, yin);
+        sl.sy.sync();
 
         if (P.mode == 1) {
             // single RHS evaluation of the state at x_in[item]
-            rhs_eval<N>(ykm, uvm, P.x_in[item], dim, P.dim_m2_cubed, k0, t, b0, b1, cur, &lam[s], P.twN, sy, active, zero_slot);
-            sy.sync();
-            if (active && s == 0) {
-                const double2* fr = cur ? b1 : b0;
+            int cur = 0;
+            rhs_eval<N>(sl.ykm, sl.uvm, P.x_in[item], P.dim, P.dim_m2_cubed, k0, sl.t, sl.b0, sl.b1, cur,
+                        &sl.lam[sl.s], P.twN, sl.sy, sl.active, sl.zero);
+            sl.sy.sync();
+            if (sl.active && sl.s == 0) {
+                const double2* fr = cur ? sl.b1 : sl.b0;
                 double* yo = P.yfinal + (size_t)item * N;
 #pragma unroll
                 for (int sg = 0; sg < 8; ++sg) {
-                    const int m = slot_mode<N>(sg, t);
-                    const double2 f = fr[sg * TG + t];
+                    const int m = slot_mode<N>(sg, sl.t);
+                    const double2 f = fr[sg * TG + sl.t];
                     yo[2 * m] = f.x;
                     yo[2 * m + 1] = f.y;
                 }
             }
-            sy.sync();
+            sl.sy.sync();
             continue;
         }
 
         const int side = P.item_side ? P.item_side[item] : (item & 1);
-        const int nsteps = P.mode == 2 ? 1 : (side == 0 ? P.nl : P.nr);
-        int status = 0, fail_at = -1;
-
-        for (int st = 0; st < nsteps; ++st) {
-            double xin, xout;
-            int gi;
-            if (P.mode == 2) {
-                xin = P.x_in[item];
-                xout = P.x_out[item];
-                gi = 0;
-            } else if (side == 0) {
-                gi = st;
-                xin = P.grid[gi];
-                xout = P.grid[gi + 1];
-            } else {
-                gi = P.nl + P.nr - st;
-                xin = P.grid[gi];
-                xout = P.grid[gi - 1];
-            }
-            const double dx = xout - xin;
-            const double xs = xin + dx * P.c[s];
-
-            bool converged = false;
-            int its_reached = 0;
-            for (int its = 0; its < P.max_its; ++its) {
-                ++its_reached;
-                rhs_eval<N>(ykm, uvm, xs, dim, P.dim_m2_cubed, k0, t, b0, b1, cur, &lam[s], P.twN, sy, active, zero_slot);
-                sy.sync();  // every stage RHS is in shared memory
-                double part = 0.0;
-                if (active) {
-#pragma unroll
-                    for (int sg = 0; sg < 8; ++sg) {
-                        double2 nv = ys[sg * TG + t];
-#pragma unroll
-                        for (int kk = 0; kk < S; ++kk) {
-                            const double w = dx * P.a[s][kk];
-                            const double2 f = ex[(size_t)(kk * 2 + cur) * K::MP + sg * TG + t];
-                            nv.x = fma(w, f.x, nv.x);
-                            nv.y = fma(w, f.y, nv.y);
-                        }
-                        const double2 old = ykm[sg * TG + t];
-                        const double ex_ = old.x - nv.x, ey_ = old.y - nv.y;
-                        part = fma(ex_, ex_, part);
-                        part = fma(ey_, ey_, part);
-                        ykm[sg * TG + t] = nv;
-                    }
-                }
-                const double tot = sweep_sum<STP, K::NW>(part, red, lt, sy);
-                const double norm2 = sqrt(tot / (double)(N * S));
-                double p10 = P.prec;
-                if (its > P.max_its / 2) p10 = P.prec * 10.0 * (2.0 * (double)its / (double)P.max_its - 0.5);
-                if (norm2 < p10) {
-                    converged = true;
-                    break;
-                }
-                if constexpr (K::NW == 1) sy.sync();  // new stage values visible to every lane
-            }
-            n_its += its_reached;
-            n_steps += 1;
-            // y += dx sum_i b_i f_i with the RHS of the last evaluation; stages restart at y
-            if (active) {
-#pragma unroll
-                for (int sg = 0; sg < 8; ++sg) {
-                    double2 y = ys[sg * TG + t];
-#pragma unroll
-                    for (int i = 0; i < S; ++i) {
-                        const double w = dx * P.b[i];
-                        const double2 f = ex[(size_t)(i * 2 + cur) * K::MP + sg * TG + t];
-                        y.x = fma(w, f.x, y.x);
-                        y.y = fma(w, f.y, y.y);
-                    }
-                    ykm[sg * TG + t] = y;
-                }
-            }
-            sy.sync();  // every group has read the old y
-            if (active && s == 0) {
-#pragma unroll
-                for (int sg = 0; sg < 8; ++sg) ys[sg * TG + t] = ykm[sg * TG + t];
-            }
-            if (P.mode == 2 && active && s == 0 && t == 0 && P.its_out)
-                P.its_out[item] = converged ? its_reached : -its_reached;
-            if (!converged) {
-                status = 1;
-                fail_at = gi;
-                break;
-            }
-        }
-        // write the final state
-        if (active && s == 0) {
-            double* yo = P.yfinal + (size_t)item * N;
-#pragma unroll
-            for (int sg = 0; sg < 8; ++sg) {
-                const int m = slot_mode<N>(sg, t);
-                const double2 y = ys[sg * TG + t];
-                yo[2 * m] = y.x;
-                yo[2 * m + 1] = y.y;
-            }
-            if (t == 0) {
-                P.status[item] = status;
-                P.fail_index[item] = fail_at;
-            }
-        }
-        sy.sync();
+        march_item<N, S>(sc, sl, k0, side, item, n_its, n_steps);
     }
-    if (lt == 0 && P.counters) {
+    if (sl.lt == 0 && P.counters) {
         atomicAdd(&P.counters[0], n_its * (unsigned long long)S);
         atomicAdd(&P.counters[1], n_its);
         atomicAdd(&P.counters[2], n_steps);
+    }
+}
+
+// ------------------------------------------------------------ batch kernel
+// Sweeps of several solves (uneven Ntau, grid sizes and dimensions) in one
+// persistent launch.  Items are grouped into Ntau classes, largest first; a
+// CTA works through the classes in that order, and inside a class every sweep
+// slot pulls its own next (solve, item) from the class counter, so sweeps of
+// different solves share a CTA.  All classes use the same 128-thread CTA and
+// the same stage count (the Gauss-Legendre tableau is a kernel parameter).
+struct BatchSolve {
+    const double* grid;
+    const double2* twN;
+    const double* yinit;  // [item][Ntau]
+    double* yfinal;
+    int* status;          // [item]
+    int* fail_index;      // [item]
+    const int* cancel;    // optional: nonzero skips the solve's remaining sweeps
+    double dim, dm2c, prec;
+    int nl, nr, max_its, ntau;
+};
+
+constexpr int kBatchMaxClasses = 4;
+
+struct BatchParams {
+    const BatchSolve* solves;
+    const int2* items;  // {solve, item = 2 column + side}, class by class
+    int n_classes;
+    int cls_ntau[kBatchMaxClasses];
+    int cls_begin[kBatchMaxClasses + 1];
+    int* cls_counter;   // [kBatchMaxClasses]
+    double a[3][3], b[3], c[3];
+    unsigned long long* counters;  // [0] RHS evaluations [1] IRK iterations [2] steps
+};
+
+// Per-sweep values of the batch kernel, staged in shared memory by the slot's
+// first thread when it takes an item.
+struct SweepScalars {
+    const double* grid;
+    const double2* twN;
+    const double* yin;
+    double* yout;
+    int* status;
+    int* fail_index;
+    double dim, dm2c, prec;
+    int nl, nr, max_its, side;
+};
+
+struct SmemScalars {
+    const SweepScalars* p;
+    const BatchParams& B;
+    __device__ __forceinline__ double dim() const { return p->dim; }
+    __device__ __forceinline__ double dm2c() const { return p->dm2c; }
+    __device__ __forceinline__ double prec() const { return p->prec; }
+    __device__ __forceinline__ int max_its() const { return p->max_its; }
+    __device__ __forceinline__ int nl() const { return p->nl; }
+    __device__ __forceinline__ int nr() const { return p->nr; }
+    __device__ __forceinline__ double grid(int i) const { return p->grid[i]; }
+    __device__ __forceinline__ const double2* twN() const { return p->twN; }
+    __device__ __forceinline__ double a(int i, int j) const { return B.a[i][j]; }
+    __device__ __forceinline__ double b(int i) const { return B.b[i]; }
+    __device__ __forceinline__ double c(int i) const { return B.c[i]; }
+    __device__ __forceinline__ int mode() const { return 0; }
+    __device__ __forceinline__ double x_in(int) const { return 0.0; }
+    __device__ __forceinline__ double x_out(int) const { return 0.0; }
+    __device__ __forceinline__ double* yout(int, int) const { return p->yout; }
+    __device__ __forceinline__ int* status(int) const { return p->status; }
+    __device__ __forceinline__ int* fail_index(int) const { return p->fail_index; }
+    __device__ __forceinline__ int* its_out(int) const { return nullptr; }
+};
+
+template <int S>
+struct BatchShape {
+    static constexpr int NT = 128;
+    static constexpr size_t max2(size_t x, size_t y) { return x > y ? x : y; }
+    static constexpr size_t SWEEPS =
+        max2(max2(MarchShape<128, S>::SMEM, MarchShape<256, S>::SMEM), max2(MarchShape<512, S>::SMEM, MarchShape<1024, S>::SMEM));
+    static constexpr int MAX_SPC = MarchShape<128, S>::SPC;
+    static constexpr size_t SMEM = SWEEPS + MAX_SPC * sizeof(SweepScalars);
+};
+
+template <int N, int S>
+__device__ __forceinline__ void batch_class(const BatchParams& B, int c, double2* smem, unsigned long long& n_its,
+                                            unsigned long long& n_steps)
+{
+    using K = MarchShape<N, S>;
+    static_assert(K::NT == BatchShape<S>::NT, "every class uses the same CTA");
+    const Slot<N, S> sl(smem, threadIdx.x);
+    if (sl.lt == 0) *sl.zero = 0;
+    SweepScalars* sp = reinterpret_cast<SweepScalars*>(reinterpret_cast<char*>(smem) + BatchShape<S>::SWEEPS) +
+                       sl.slot_id;
+    const SmemScalars sc{sp, B};
+    const int n = B.cls_begin[c + 1] - B.cls_begin[c];
+    unsigned long long c_its = 0, c_steps = 0;  // this slot's sweeps in this class
+    for (;;) {
+        if (sl.lt == 0) {
+            int i = atomicAdd(&B.cls_counter[c], 1);
+            while (i < n) {
+                const int2 it = B.items[B.cls_begin[c] + i];
+                const BatchSolve& so = B.solves[it.x];
+                if (so.cancel && *(const volatile int*)so.cancel) {  // the solve no longer needs this sweep
+                    i = atomicAdd(&B.cls_counter[c], 1);
+                    continue;
+                }
+                sp->grid = so.grid;
+                sp->twN = so.twN;
+                sp->yin = so.yinit + (size_t)it.y * N;
+                sp->yout = so.yfinal + (size_t)it.y * N;
+                sp->status = so.status + it.y;
+                sp->fail_index = so.fail_index + it.y;
+                sp->dim = so.dim;
+                sp->dm2c = so.dm2c;
+                sp->prec = so.prec;
+                sp->nl = so.nl;
+                sp->nr = so.nr;
+                sp->max_its = so.max_its;
+                sp->side = it.y & 1;
+                break;
+            }
+            *sl.item_slot = i;
+        }
+        sl.sy.sync();
+        const int item = *sl.item_slot;
+        if (item >= n) break;
+        const double* yin = sp->yin;
+        const double k0 = 2.0 * kPi / yin[4];
+        load_state<N, S>(sl, yin);
+        sl.sy.sync();
+        march_item<N, S>(sc, sl, k0, sp->side, item, c_its, c_steps);
+    }
+    if (sl.lt == 0) {  // one thread per slot reports the slot's work
+        n_its += c_its;
+        n_steps += c_steps;
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(128, 2) march_batch_kernel(BatchParams B)
+{
+    extern __shared__ double2 smem[];
+    unsigned long long n_its = 0, n_steps = 0;
+    for (int c = 0; c < B.n_classes; ++c) {
+        switch (B.cls_ntau[c]) {
+            case 1024: batch_class<1024, S>(B, c, smem, n_its, n_steps); break;
+            case 512: batch_class<512, S>(B, c, smem, n_its, n_steps); break;
+            case 256: batch_class<256, S>(B, c, smem, n_its, n_steps); break;
+            case 128: batch_class<128, S>(B, c, smem, n_its, n_steps); break;
+            default: break;
+        }
+        __syncthreads();  // the next class partitions shared memory differently
+    }
+    if (n_steps && B.counters) {
+        atomicAdd(&B.counters[0], n_its * (unsigned long long)S);
+        atomicAdd(&B.counters[1], n_its);
+        atomicAdd(&B.counters[2], n_steps);
     }
 }
 

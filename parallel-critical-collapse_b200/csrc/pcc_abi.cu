@@ -16,54 +16,9 @@
 
 #include "pcc.h"
 #include "pcc_internal.h"
+#include "pcc_objects.h"
 
 using namespace pcc;
-
-struct pcc_ctx {
-    int device = 0;
-    int sms = 0;
-    cudaStream_t stream = nullptr;
-    std::string last_error;
-    std::vector<pcc_solve*> solves;  // live solves; destroyed with the context
-    // LU workspace (grown on demand)
-    void* lu_work = nullptr;
-    size_t lu_work_bytes = 0;
-};
-
-struct pcc_solve {
-    pcc_ctx* ctx = nullptr;
-    pcc_solve_desc d{};
-    int nn = 0;      // Nnewton
-    int ngrid = 0;   // nl + nr + 1
-    int stages = 2;
-    double a[3][3]{}, b[3]{}, c[3]{};
-    double dm2c = 0.0;
-    std::vector<double> grid;
-    // device buffers
-    double* d_grid = nullptr;
-    double2* d_tw = nullptr;
-    double* d_in0 = nullptr;
-    double* d_out0 = nullptr;
-    double* d_J = nullptr;
-    double* d_yinit = nullptr;    // [2*(nn+1)][N]
-    double* d_yfinal = nullptr;   // [2*(nn+1)][N]
-    double* d_outc = nullptr;     // [nn+1][nn]
-    int* d_status = nullptr;      // [2*(nn+1)] march status
-    int* d_fail = nullptr;        // [2*(nn+1)]
-    int* d_cstatus = nullptr;     // [nn+1] epilogue status
-    int* d_counters_i = nullptr;  // [4] work counters
-    unsigned long long* d_counters = nullptr;  // [4] march counters
-    double* d_scratch = nullptr;
-    int scratch_ctas = 0;
-    int* d_item_side = nullptr;   // pcc_sweep
-    double* d_xs = nullptr;       // pcc_sweep / test entry points (x_in, x_out)
-    int* d_its = nullptr;
-    // last asynchronous build
-    int pend_c0 = 0, pend_c1 = 0;
-    bool pending = false;
-    cudaEvent_t ev[5]{};
-    MarchLaunchInfo last_launch{};
-};
 
 cudaStream_t pcc_ctx_stream(pcc_ctx* ctx) { return ctx->stream; }
 int pcc_ctx_device(pcc_ctx* ctx) { return ctx->device; }
@@ -83,21 +38,6 @@ const char* kStatusNames[] = {"PCC_OK",
                               "PCC_ERR_UNSUPPORTED",
                               "PCC_ERR_NEWTON_NO_CONVERGENCE",
                               "PCC_ERR_BUSY"};
-
-pcc_status fail(pcc_ctx* ctx, pcc_status s, const std::string& msg)
-{
-    if (ctx) ctx->last_error = msg;
-    return s;
-}
-
-#define PCC_CUDA(ctx, call)                                                                          \
-    do {                                                                                             \
-        cudaError_t _e = (call);                                                                     \
-        if (_e != cudaSuccess) {                                                                     \
-            return fail((ctx), _e == cudaErrorMemoryAllocation ? PCC_ERR_OOM : PCC_ERR_CUDA,         \
-                        std::string(#call) + ": " + cudaGetErrorString(_e));                         \
-        }                                                                                            \
-    } while (0)
 
 // Gauss-Legendre tableaux exactly as ODEStepper.cpp:27-79 builds them.
 int tableau(int scheme, double a[3][3], double b[3], double c[3])
@@ -216,18 +156,8 @@ MarchParams march_params(pcc_solve* s)
     return P;
 }
 
-// Enqueues the build pipeline for columns [c0, c1) reading d_in0 (and d_out0
-// for the differences when fd is set).  Events bracket the stages.
-pcc_status enqueue_columns(pcc_solve* s, int c0, int c1, bool fd, double* d_J)
+BoundaryParams boundary_params(pcc_solve* s, int c0)
 {
-    pcc_ctx* ctx = s->ctx;
-    cudaStream_t st = ctx->stream;
-    const int ncols = c1 - c0;
-    const int items = 2 * ncols;
-    PCC_CUDA(ctx, cudaMemsetAsync(s->d_counters_i, 0, 4 * sizeof(int), st));
-    PCC_CUDA(ctx, cudaMemsetAsync(s->d_counters, 0, 4 * sizeof(unsigned long long), st));
-    PCC_CUDA(ctx, cudaEventRecord(s->ev[0], st));
-
     BoundaryParams B{};
     B.ntau = s->d.ntau;
     B.nn = s->nn;
@@ -246,29 +176,60 @@ pcc_status enqueue_columns(pcc_solve* s, int c0, int c1, bool fd, double* d_J)
     B.status = s->d_cstatus;
     B.scratch = s->d_scratch;
     B.tw = s->d_tw;
+    return B;
+}
 
+// Boundary data of columns [c0, c1) from d_in0 -> d_yinit (and cleared counters).
+pcc_status enqueue_prologue(pcc_solve* s, int c0, int c1, cudaStream_t st)
+{
+    pcc_ctx* ctx = s->ctx;
+    const int items = 2 * (c1 - c0);
+    PCC_CUDA(ctx, cudaMemsetAsync(s->d_counters_i, 0, 4 * sizeof(int), st));
+    PCC_CUDA(ctx, cudaMemsetAsync(s->d_counters, 0, 4 * sizeof(unsigned long long), st));
+    BoundaryParams B = boundary_params(s, c0);
     B.n_items = items;
     B.work_counter = s->d_counters_i + 0;
     PCC_CUDA(ctx, launch_prologue(B, boundary_ctas(s, items), st));
-    PCC_CUDA(ctx, cudaEventRecord(s->ev[1], st));
+    return PCC_OK;
+}
 
+// Mismatch of columns [c0, c1) -> d_outc, then (fd) J's columns [c0, min(c1, nn)).
+pcc_status enqueue_epilogue(pcc_solve* s, int c0, int c1, bool fd, double* d_J, cudaStream_t st)
+{
+    pcc_ctx* ctx = s->ctx;
+    const int ncols = c1 - c0;
+    BoundaryParams B = boundary_params(s, c0);
+    B.n_items = ncols;
+    B.work_counter = s->d_counters_i + 2;
+    PCC_CUDA(ctx, launch_epilogue(B, boundary_ctas(s, ncols), st));
+    if (fd) {
+        // the base column (index nn) has no difference
+        const int nfd = (c1 > s->nn ? s->nn : c1) - c0;
+        if (nfd > 0) PCC_CUDA(ctx, launch_fd(s->d_outc, s->d_out0, d_J, s->nn, c0, nfd, s->d.eps_newton, st));
+    }
+    return PCC_OK;
+}
+
+// Enqueues the build pipeline for columns [c0, c1) reading d_in0 (and d_out0
+// for the differences when fd is set).  Events bracket the stages.
+pcc_status enqueue_columns(pcc_solve* s, int c0, int c1, bool fd, double* d_J)
+{
+    pcc_ctx* ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    PCC_CUDA(ctx, cudaEventRecord(s->ev[0], st));
+    pcc_status r = enqueue_prologue(s, c0, c1, st);
+    if (r != PCC_OK) return r;
+    PCC_CUDA(ctx, cudaEventRecord(s->ev[1], st));
     MarchParams P = march_params(s);
-    P.n_items = items;
+    P.n_items = 2 * (c1 - c0);
     P.mode = 0;
     P.yinit = s->d_yinit;
     P.yfinal = s->d_yfinal;
     P.work_counter = s->d_counters_i + 1;
     PCC_CUDA(ctx, launch_march(s->d.ntau, s->stages, P, 0, st, &s->last_launch));
     PCC_CUDA(ctx, cudaEventRecord(s->ev[2], st));
-
-    B.n_items = ncols;
-    B.work_counter = s->d_counters_i + 2;
-    PCC_CUDA(ctx, launch_epilogue(B, boundary_ctas(s, ncols), st));
-    if (fd) {
-        // columns [c0, min(c1, nn)) of J; the base column (index nn) has no difference
-        const int nfd = (c1 > s->nn ? s->nn : c1) - c0;
-        if (nfd > 0) PCC_CUDA(ctx, launch_fd(s->d_outc, s->d_out0, d_J, s->nn, c0, nfd, s->d.eps_newton, st));
-    }
+    r = enqueue_epilogue(s, c0, c1, fd, d_J, st);
+    if (r != PCC_OK) return r;
     PCC_CUDA(ctx, cudaEventRecord(s->ev[3], st));
     return PCC_OK;
 }
@@ -325,6 +286,197 @@ pcc_status collect(pcc_solve* s, int c0, int c1, pcc_stats* stats)
     return result;
 }
 
+// Grows a device buffer and its pinned host staging buffer to `bytes`.
+pcc_status batch_tables(pcc_ctx* ctx, size_t bytes)
+{
+    if (ctx->d_batch_bytes < bytes) {
+        if (ctx->d_batch) cudaFree(ctx->d_batch);
+        ctx->d_batch = nullptr;
+        ctx->d_batch_bytes = 0;
+        PCC_CUDA(ctx, cudaMalloc(&ctx->d_batch, bytes));
+        ctx->d_batch_bytes = bytes;
+    }
+    if (ctx->h_batch_bytes < bytes) {
+        if (ctx->h_batch) cudaFreeHost(ctx->h_batch);
+        ctx->h_batch = nullptr;
+        ctx->h_batch_bytes = 0;
+        PCC_CUDA(ctx, cudaMallocHost(&ctx->h_batch, bytes));
+        ctx->h_batch_bytes = bytes;
+    }
+    for (auto& ev : ctx->bev)
+        if (!ev) PCC_CUDA(ctx, cudaEventCreate(&ev));
+    return PCC_OK;
+}
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Builds the item table of a batch march over columns [0, ncols[i]) of every
+// solve: Ntau classes in decreasing order, inside a class the longest sweeps
+// first (longest-processing-time order), ties by solve and item.
+void batch_items(const std::vector<pcc_solve*>& v, const std::vector<int>& ncols, BatchParams& B,
+                 std::vector<int2>& items)
+{
+    static const int kOrder[kBatchMaxClasses] = {1024, 512, 256, 128};
+    items.clear();
+    B.n_classes = 0;
+    for (int n : kOrder) {
+        std::vector<std::pair<int, int2>> cls;  // (steps, item)
+        for (size_t i = 0; i < v.size(); ++i) {
+            if (v[i]->d.ntau != n) continue;
+            for (int k = 0; k < 2 * ncols[i]; ++k)
+                cls.push_back({(k & 1) ? v[i]->d.nr : v[i]->d.nl, make_int2((int)i, k)});
+        }
+        if (cls.empty()) continue;
+        std::stable_sort(cls.begin(), cls.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+        B.cls_ntau[B.n_classes] = n;
+        B.cls_begin[B.n_classes] = (int)items.size();
+        for (auto& c : cls) items.push_back(c.second);
+        B.n_classes += 1;
+    }
+    B.cls_begin[B.n_classes] = (int)items.size();
+}
+
+// One persistent launch over the sweeps of columns [0, ncols[i]) of every
+// solve in v (all batch-supported, same stage count), on stream st.
+pcc_status enqueue_batch_march(pcc_ctx* ctx, const std::vector<pcc_solve*>& v, const std::vector<int>& ncols,
+                               cudaStream_t st)
+{
+    BatchParams B{};
+    std::vector<int2> items;
+    batch_items(v, ncols, B, items);
+    const size_t o_solves = 0;
+    const size_t o_items = align_up(o_solves + v.size() * sizeof(BatchSolve), 16);
+    const size_t o_cls = align_up(o_items + items.size() * sizeof(int2), 16);
+    const size_t o_cnt = align_up(o_cls + kBatchMaxClasses * sizeof(int), 16);
+    const size_t bytes = o_cnt + 4 * sizeof(unsigned long long);
+    pcc_status r = batch_tables(ctx, bytes);
+    if (r != PCC_OK) return r;
+    char* h = static_cast<char*>(ctx->h_batch);
+    char* d = static_cast<char*>(ctx->d_batch);
+    auto* hs = reinterpret_cast<BatchSolve*>(h + o_solves);
+    for (size_t i = 0; i < v.size(); ++i) {
+        pcc_solve* s = v[i];
+        BatchSolve& b = hs[i];
+        b.grid = s->d_grid;
+        b.twN = s->d_tw;
+        b.yinit = s->d_yinit;
+        b.yfinal = s->d_yfinal;
+        b.status = s->d_status;
+        b.fail_index = s->d_fail;
+        b.cancel = s->d_cancel;
+        b.dim = s->d.dim;
+        b.dm2c = s->dm2c;
+        b.prec = s->d.prec_irk;
+        b.nl = s->d.nl;
+        b.nr = s->d.nr;
+        b.max_its = s->d.max_irk;
+        b.ntau = s->d.ntau;
+    }
+    std::memcpy(h + o_items, items.data(), items.size() * sizeof(int2));
+    std::memset(h + o_cls, 0, o_cnt - o_cls + 4 * sizeof(unsigned long long));
+    PCC_CUDA(ctx, cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
+    B.solves = reinterpret_cast<const BatchSolve*>(d + o_solves);
+    B.items = reinterpret_cast<const int2*>(d + o_items);
+    B.cls_counter = reinterpret_cast<int*>(d + o_cls);
+    B.counters = reinterpret_cast<unsigned long long*>(d + o_cnt);
+    ctx->batch_cnt_off = o_cnt;
+    const pcc_solve* s0 = v[0];
+    for (int i = 0; i < 3; ++i) {
+        B.b[i] = s0->b[i];
+        B.c[i] = s0->c[i];
+        for (int j = 0; j < 3; ++j) B.a[i][j] = s0->a[i][j];
+    }
+    PCC_CUDA(ctx, cudaEventRecord(ctx->bev[0], st));
+    PCC_CUDA(ctx, launch_march_batch(B, 0, st, &ctx->batch_launch));
+    PCC_CUDA(ctx, cudaEventRecord(ctx->bev[1], st));
+    return PCC_OK;
+}
+
+// Reads the counters and timing of the last batch march (stream synchronised).
+void batch_stats(pcc_ctx* ctx, const std::vector<pcc_solve*>& v, const std::vector<int>& ncols, pcc_stats* stats)
+{
+    if (!stats) return;
+    std::memset(stats, 0, sizeof(*stats));
+    (void)v;
+    unsigned long long cnt[4] = {0, 0, 0, 0};
+    cudaMemcpy(cnt, static_cast<char*>(ctx->d_batch) + ctx->batch_cnt_off, 3 * sizeof(unsigned long long),
+               cudaMemcpyDeviceToHost);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->bev[0], ctx->bev[1]);
+    stats->rhs_evals = (long long)cnt[0];
+    stats->irk_iterations = (long long)cnt[1];
+    stats->irk_steps = (long long)cnt[2];
+    long long shoots = 0;
+    for (int c : ncols) shoots += c;
+    stats->shoots = shoots;
+    stats->ms_sweep = ms;
+    stats->ms_total = ms;
+    stats->fail_column = -1;
+    stats->fail_grid_index = -1;
+    stats->sweep_ctas = ctx->batch_launch.ctas;
+}
+
+// Finds the first failing sweep or column of a solve's last shoots.
+void solve_failure(pcc_solve* s, int ncols, int* col, int* side, int* idx)
+{
+    *col = *side = *idx = -1;
+    std::vector<int> st(2 * ncols), fi(2 * ncols), cs(ncols);
+    if (cudaMemcpy(st.data(), s->d_status, st.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return;
+    cudaMemcpy(fi.data(), s->d_fail, fi.size() * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(cs.data(), s->d_cstatus, cs.size() * sizeof(int), cudaMemcpyDeviceToHost);
+    for (int i = 0; i < 2 * ncols; ++i)
+        if (st[i] != 0) {
+            *col = i / 2;
+            *side = i & 1;
+            *idx = fi[i];
+            return;
+        }
+    for (int i = 0; i < ncols; ++i)
+        if (cs[i] != 0) {
+            *col = i;
+            return;
+        }
+}
+
+// After the march of one Newton iteration (base column nn and columns 0..nn-1):
+// mismatches, the device-side check of NewtonSolver.cpp:300-325, J, the
+// Newton solve and the damped update, all on stream st.
+pcc_status enqueue_newton_tail(pcc_solve* s, pcc_precision prec, cudaStream_t st, int* lu_steps, int* lu_fallback)
+{
+    pcc_ctx* ctx = s->ctx;
+    const int nn = s->nn;
+    pcc_status r = enqueue_epilogue(s, 0, nn + 1, false, nullptr, st);
+    if (r != PCC_OK) return r;
+    PCC_CUDA(ctx, cudaMemcpyAsync(s->d_out0, s->d_outc + (size_t)nn * nn, nn * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, st));
+    PCC_CUDA(ctx, launch_newton_check(s->d_newton, s->d_out0, nn, s->d_status, s->d_cstatus, s->d.prec_newton,
+                                      s->d_rhs, st));
+    PCC_CUDA(ctx, launch_fd(s->d_outc, s->d_out0, s->d_J, nn, 0, nn, s->d.eps_newton, st));
+    *lu_steps = -1;
+    *lu_fallback = 0;
+    if (prec == PCC_PREC_MIXED) {
+        double resid = -1.0;
+        PCC_CUDA(ctx, lu_solve_mixed(s->d_J, s->d_rhs, s->d_dx, nn, s->d_luw, lu_mixed_work_bytes(nn), s->d_ipiv,
+                                     s->d_info, 30, 1e-15, lu_steps, &resid, st));
+    } else {
+        PCC_CUDA(ctx, lu_solve_fp64(s->d_J, s->d_rhs, s->d_dx, nn, nullptr, s->d_ipiv, s->d_info, st));
+    }
+    PCC_CUDA(ctx, launch_newton_update(s->d_newton, s->d_in0, s->d_in0old, s->d_dx, s->d_info, nn,
+                                       s->d.slow_error, s->d.max_newton, st));
+    return PCC_OK;
+}
+
+void newton_state_from_dev(const NewtonDev& nd, pcc_newton_state* out)
+{
+    out->iterations = nd.its;
+    out->code = nd.state;
+    out->err = nd.err;
+    out->err_old = nd.err_old;
+    out->fail_column = out->fail_side = out->fail_grid_index = -1;
+    out->lu_refinement_steps = -1;
+    out->lu_fell_back = 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -361,8 +513,13 @@ pcc_status pcc_ctx_destroy(pcc_ctx* ctx)
     if (!ctx) return PCC_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    server_shutdown(ctx);
     while (!ctx->solves.empty()) pcc_solve_destroy(ctx->solves.back());
     if (ctx->lu_work) cudaFree(ctx->lu_work);
+    if (ctx->d_batch) cudaFree(ctx->d_batch);
+    if (ctx->h_batch) cudaFreeHost(ctx->h_batch);
+    for (auto& ev : ctx->bev)
+        if (ev) cudaEventDestroy(ev);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return PCC_OK;
@@ -393,6 +550,7 @@ pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve*
     do {                                                                                                     \
         cudaError_t _e = cudaMalloc((void**)&(ptr), (bytes));                                                \
         if (_e != cudaSuccess) return cleanup(PCC_ERR_OOM, std::string("cudaMalloc ") + #ptr + ": " + cudaGetErrorString(_e)); \
+        s->footprint += (bytes);                                                                             \
     } while (0)
     ALLOC(s->d_grid, s->ngrid * sizeof(double));
     ALLOC(s->d_tw, n * sizeof(double2));
@@ -411,10 +569,20 @@ pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve*
     ALLOC(s->d_item_side, 2 * cols * sizeof(int));
     ALLOC(s->d_xs, 4 * cols * sizeof(double));
     ALLOC(s->d_its, 2 * cols * sizeof(int));
+    ALLOC(s->d_newton, sizeof(NewtonDev));
+    ALLOC(s->d_in0old, nn * sizeof(double));
+    ALLOC(s->d_rhs, nn * sizeof(double));
+    ALLOC(s->d_dx, nn * sizeof(double));
+    ALLOC(s->d_ipiv, nn * sizeof(int));
+    ALLOC(s->d_info, 2 * sizeof(int));
+    ALLOC(s->d_luw, lu_mixed_work_bytes(nn));
+    ALLOC(s->d_cancel, sizeof(int));
 #undef ALLOC
     const std::vector<double2> tw = twiddles(n);
     cudaError_t e = cudaMemcpy(s->d_tw, tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s->d_grid, s->grid.data(), s->ngrid * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(s->d_cancel, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(s->d_newton, 0, sizeof(NewtonDev));
     for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&s->ev[i]);
     if (e != cudaSuccess) return cleanup(PCC_ERR_CUDA, cudaGetErrorString(e));
     ctx->solves.push_back(s);
@@ -431,7 +599,8 @@ pcc_status pcc_solve_destroy(pcc_solve* s)
     cudaStreamSynchronize(s->ctx->stream);
     void* ptrs[] = {s->d_grid, s->d_tw, s->d_in0, s->d_out0, s->d_J, s->d_yinit, s->d_yfinal, s->d_outc,
                     s->d_status, s->d_fail, s->d_cstatus, s->d_counters_i, s->d_counters, s->d_scratch,
-                    s->d_item_side, s->d_xs, s->d_its};
+                    s->d_item_side, s->d_xs, s->d_its, s->d_newton, s->d_in0old, s->d_rhs, s->d_dx,
+                    s->d_ipiv, s->d_info, s->d_luw, s->d_cancel};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& ev : s->ev)
@@ -902,6 +1071,217 @@ pcc_status pcc_fp64_peak(pcc_ctx* ctx, double* tflops)
     if (!ctx || !tflops) return PCC_ERR_INVALID_ARG;
     PCC_CUDA(ctx, cudaSetDevice(ctx->device));
     PCC_CUDA(ctx, fp64_peak_probe(tflops, ctx->stream));
+    return PCC_OK;
+}
+
+// ------------------------------------------------ batches and device Newton
+
+pcc_status pcc_jacobian_batch(pcc_ctx* ctx, int count, pcc_solve* const* solves, const double* const* in0,
+                              const double* const* out0, double* const* J, pcc_stats* stats)
+{
+    if (!ctx || count < 1 || !solves || !in0 || !out0 || !J) return PCC_ERR_INVALID_ARG;
+    std::vector<pcc_solve*> v(solves, solves + count);
+    for (int i = 0; i < count; ++i) {
+        if (!v[i] || v[i]->ctx != ctx || !in0[i] || !out0[i] || !J[i]) return PCC_ERR_INVALID_ARG;
+        if (!march_batch_supported(v[i]->d.ntau, v[i]->stages))
+            return fail(ctx, PCC_ERR_UNSUPPORTED, "batch: Ntau must be 128..1024 with 2 IRK stages");
+        for (int j = 0; j < i; ++j)
+            if (v[j] == v[i]) return fail(ctx, PCC_ERR_INVALID_ARG, "batch: a solve is listed twice");
+    }
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    std::vector<int> ncols(count);
+    for (int i = 0; i < count; ++i) {
+        pcc_solve* s = v[i];
+        ncols[i] = s->nn;
+        PCC_CUDA(ctx, cudaMemcpyAsync(s->d_in0, in0[i], s->nn * sizeof(double), cudaMemcpyHostToDevice, st));
+        PCC_CUDA(ctx, cudaMemcpyAsync(s->d_out0, out0[i], s->nn * sizeof(double), cudaMemcpyHostToDevice, st));
+        pcc_status r = enqueue_prologue(s, 0, s->nn, st);
+        if (r != PCC_OK) return r;
+    }
+    pcc_status r = enqueue_batch_march(ctx, v, ncols, st);
+    if (r != PCC_OK) return r;
+    for (int i = 0; i < count; ++i) {
+        pcc_solve* s = v[i];
+        r = enqueue_epilogue(s, 0, s->nn, true, s->d_J, st);
+        if (r != PCC_OK) return r;
+        PCC_CUDA(ctx, cudaMemcpyAsync(J[i], s->d_J, (size_t)s->nn * s->nn * sizeof(double), cudaMemcpyDeviceToHost,
+                                      st));
+    }
+    PCC_CUDA(ctx, cudaStreamSynchronize(st));
+    batch_stats(ctx, v, ncols, stats);
+    for (int i = 0; i < count; ++i) {
+        int col, side, idx;
+        solve_failure(v[i], ncols[i], &col, &side, &idx);
+        if (col >= 0) {
+            char buf[160];
+            std::snprintf(buf, sizeof buf, "batch solve %d: %s at column %d side %d grid index %d", i,
+                          side >= 0 ? "IRK no convergence" : "Delta mismatch", col, side, idx);
+            if (stats) {
+                stats->fail_column = col;
+                stats->fail_side = side < 0 ? 0 : side;
+                stats->fail_grid_index = idx;
+            }
+            return fail(ctx, side >= 0 ? PCC_ERR_IRK_NO_CONVERGENCE : PCC_ERR_DELTA_MISMATCH, buf);
+        }
+    }
+    return PCC_OK;
+}
+
+pcc_status pcc_newton_begin(pcc_solve* s, const double* in0)
+{
+    if (!s || !in0) return PCC_ERR_INVALID_ARG;
+    pcc_ctx* ctx = s->ctx;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    PCC_CUDA(ctx, cudaMemcpyAsync(s->d_in0, in0, s->nn * sizeof(double), cudaMemcpyHostToDevice, st));
+    PCC_CUDA(ctx, launch_newton_reset(s->d_newton, s->d_in0, s->d_in0old, s->nn, st));
+    PCC_CUDA(ctx, cudaMemsetAsync(s->d_cancel, 0, sizeof(int), st));
+    PCC_CUDA(ctx, cudaStreamSynchronize(st));
+    s->h_newton = kNewtonRunning;
+    return PCC_OK;
+}
+
+pcc_status pcc_newton_iterate(pcc_ctx* ctx, int count, pcc_solve* const* solves, pcc_precision prec,
+                              pcc_newton_state* states, pcc_stats* stats)
+{
+    if (!ctx || count < 1 || !solves) return PCC_ERR_INVALID_ARG;
+    if (prec != PCC_PREC_FP64 && prec != PCC_PREC_MIXED) return PCC_ERR_INVALID_ARG;
+    for (int i = 0; i < count; ++i) {
+        if (!solves[i] || solves[i]->ctx != ctx) return PCC_ERR_INVALID_ARG;
+        for (int j = 0; j < i; ++j)
+            if (solves[j] == solves[i]) return fail(ctx, PCC_ERR_INVALID_ARG, "a solve is listed twice");
+    }
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    std::vector<pcc_solve*> run, batch, single;
+    for (int i = 0; i < count; ++i)
+        if (solves[i]->h_newton == kNewtonRunning) {
+            run.push_back(solves[i]);
+            (march_batch_supported(solves[i]->d.ntau, solves[i]->stages) ? batch : single).push_back(solves[i]);
+        }
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    std::vector<int> steps(count, -1), fb(count, 0);
+    if (!run.empty()) {
+        for (pcc_solve* s : run) {
+            pcc_status r = enqueue_prologue(s, 0, s->nn + 1, st);
+            if (r != PCC_OK) return r;
+        }
+        if (!batch.empty()) {
+            std::vector<int> ncols;
+            for (pcc_solve* s : batch) ncols.push_back(s->nn + 1);
+            pcc_status r = enqueue_batch_march(ctx, batch, ncols, st);
+            if (r != PCC_OK) return r;
+        }
+        for (pcc_solve* s : single) {
+            MarchParams P = march_params(s);
+            P.n_items = 2 * (s->nn + 1);
+            P.mode = 0;
+            P.yinit = s->d_yinit;
+            P.yfinal = s->d_yfinal;
+            P.work_counter = s->d_counters_i + 1;
+            PCC_CUDA(ctx, launch_march(s->d.ntau, s->stages, P, 0, st, &s->last_launch));
+        }
+        for (int i = 0; i < count; ++i) {
+            pcc_solve* s = solves[i];
+            if (s->h_newton != kNewtonRunning) continue;
+            pcc_status r = enqueue_newton_tail(s, prec, st, &steps[i], &fb[i]);
+            if (r != PCC_OK) return r;
+        }
+        PCC_CUDA(ctx, cudaStreamSynchronize(st));
+        if (stats && !batch.empty()) {
+            std::vector<int> ncols;
+            for (pcc_solve* s : batch) ncols.push_back(s->nn + 1);
+            batch_stats(ctx, batch, ncols, stats);
+        }
+        if (stats) {
+            for (pcc_solve* s : single) {
+                unsigned long long cnt[4];
+                PCC_CUDA(ctx, cudaMemcpy(cnt, s->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+                stats->rhs_evals += (long long)cnt[0];
+                stats->irk_iterations += (long long)cnt[1];
+                stats->irk_steps += (long long)cnt[2];
+                stats->shoots += s->nn + 1;
+            }
+        }
+    }
+    for (int i = 0; i < count; ++i) {
+        pcc_solve* s = solves[i];
+        NewtonDev nd{};
+        PCC_CUDA(ctx, cudaMemcpy(&nd, s->d_newton, sizeof(nd), cudaMemcpyDeviceToHost));
+        s->h_newton = nd.state;
+        if (states) {
+            newton_state_from_dev(nd, &states[i]);
+            states[i].lu_refinement_steps = steps[i];
+            int info[2] = {0, 0};
+            PCC_CUDA(ctx, cudaMemcpy(info, s->d_info, sizeof(info), cudaMemcpyDeviceToHost));
+            states[i].lu_fell_back = prec == PCC_PREC_MIXED ? info[1] : 0;
+            if (nd.state == kNewtonIrkFailed || nd.state == kNewtonDeltaMismatch)
+                solve_failure(s, s->nn + 1, &states[i].fail_column, &states[i].fail_side,
+                              &states[i].fail_grid_index);
+        }
+    }
+    return PCC_OK;
+}
+
+pcc_status pcc_newton_result(pcc_solve* s, double* in0_out, pcc_newton_state* state)
+{
+    if (!s || !in0_out) return PCC_ERR_INVALID_ARG;
+    pcc_ctx* ctx = s->ctx;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    PCC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    NewtonDev nd{};
+    PCC_CUDA(ctx, cudaMemcpy(&nd, s->d_newton, sizeof(nd), cudaMemcpyDeviceToHost));
+    // a solve stopped by the divergence safeguard returns its last improving iterate (NewtonSolver.cpp:317-321)
+    const double* src = nd.state == kNewtonStopped ? s->d_in0old : s->d_in0;
+    PCC_CUDA(ctx, cudaMemcpy(in0_out, src, s->nn * sizeof(double), cudaMemcpyDeviceToHost));
+    if (state) newton_state_from_dev(nd, state);
+    return PCC_OK;
+}
+
+pcc_status pcc_newton_solve(pcc_ctx* ctx, int count, pcc_solve* const* solves, double* const* in0,
+                            pcc_precision prec, pcc_newton_state* states, pcc_stats* stats)
+{
+    if (!ctx || count < 1 || !solves || !in0) return PCC_ERR_INVALID_ARG;
+    for (int i = 0; i < count; ++i) {
+        if (!solves[i] || !in0[i]) return PCC_ERR_INVALID_ARG;
+        pcc_status r = pcc_newton_begin(solves[i], in0[i]);
+        if (r != PCC_OK) return r;
+    }
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    std::vector<pcc_newton_state> cur(count);
+    for (;;) {
+        bool any = false;
+        for (int i = 0; i < count; ++i) any = any || solves[i]->h_newton == kNewtonRunning;
+        if (!any) break;
+        pcc_stats it{};
+        pcc_status r = pcc_newton_iterate(ctx, count, solves, prec, cur.data(), &it);
+        if (r != PCC_OK) return r;
+        if (stats) {
+            stats->rhs_evals += it.rhs_evals;
+            stats->irk_iterations += it.irk_iterations;
+            stats->irk_steps += it.irk_steps;
+            stats->shoots += it.shoots;
+            stats->ms_sweep += it.ms_sweep;
+            stats->ms_total += it.ms_total;
+            stats->sweep_ctas = it.sweep_ctas;
+        }
+        if (states)
+            for (int i = 0; i < count; ++i) states[i] = cur[i];
+    }
+    for (int i = 0; i < count; ++i) {
+        pcc_newton_state fin{};
+        pcc_status r = pcc_newton_result(solves[i], in0[i], &fin);
+        if (r != PCC_OK) return r;
+        if (states) {
+            fin.fail_column = cur[i].fail_column;
+            fin.fail_side = cur[i].fail_side;
+            fin.fail_grid_index = cur[i].fail_grid_index;
+            fin.lu_refinement_steps = cur[i].lu_refinement_steps;
+            fin.lu_fell_back = cur[i].lu_fell_back;
+            states[i] = fin;
+        }
+    }
     return PCC_OK;
 }
 

@@ -33,6 +33,37 @@ cudaError_t launch_march(int ntau, int stages, const MarchParams& P, int max_cta
                          MarchLaunchInfo* info);
 bool march_supported(int ntau, int stages);
 
+// Sweeps of several solves in one persistent launch (march_batch_kernel):
+// Ntau in {128, 256, 512, 1024} with 2 stages.  B.cls_counter must be zero.
+cudaError_t launch_march_batch(const BatchParams& B, int max_ctas, cudaStream_t st, MarchLaunchInfo* info);
+bool march_batch_supported(int ntau, int stages);
+
+// Device-resident Newton state of one solve (newton.cu).
+enum NewtonStateCode {
+    kNewtonRunning = 0,
+    kNewtonConverged = 1,     // err < PrecisionNewton
+    kNewtonStopped = 2,       // five mismatch increases: the last improving iterate is the result
+    kNewtonMaxIter = 3,       // MaxIterNewton iterations without convergence
+    kNewtonIrkFailed = 4,     // a sweep's IRK iteration did not converge
+    kNewtonDeltaMismatch = 5, // the two sides' Delta differ
+    kNewtonSingular = 6       // zero pivot in the Newton solve
+};
+
+struct NewtonDev {
+    double err;       // mismatch RMS of the last base shoot
+    double err_old;   // of the one before
+    int its;          // iterations whose base shoot was evaluated
+    int inc_count;    // mismatch increases since the last improvement
+    int state;        // NewtonStateCode
+    int fail_item;
+};
+
+cudaError_t launch_newton_reset(NewtonDev* nd, const double* in0, double* in0old, int nn, cudaStream_t st);
+cudaError_t launch_newton_check(NewtonDev* nd, const double* out0, int nn, const int* sweep_status,
+                                const int* col_status, double tol, double* rhs, cudaStream_t st);
+cudaError_t launch_newton_update(NewtonDev* nd, double* in0, double* in0old, const double* dx, const int* lu_info,
+                                 int nn, double slow_error, int max_its, cudaStream_t st);
+
 // LU helpers (lu.cu)
 cudaError_t lu_solve_fp64(const double* dA, const double* db, double* dx, int n, double* work, int* ipiv,
                           int* info, cudaStream_t st);

@@ -1,0 +1,101 @@
+// pcc_objects.h -- the opaque objects of include/pcc.h and the error helpers
+// shared by the translation units that implement the C ABI.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "pcc.h"
+#include "pcc_internal.h"
+
+namespace pcc {
+struct Server;
+}
+
+struct pcc_ctx {
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    std::vector<pcc_solve*> solves;  // live solves; destroyed with the context
+    // LU workspace (grown on demand)
+    void* lu_work = nullptr;
+    size_t lu_work_bytes = 0;
+    // batch launch tables (grown on demand): BatchSolve[], int2 items[], class counters, march counters
+    void* d_batch = nullptr;
+    size_t d_batch_bytes = 0;
+    void* h_batch = nullptr;  // pinned staging of the same layout
+    size_t h_batch_bytes = 0;
+    size_t batch_cnt_off = 0; // offset of the march counters in d_batch
+    cudaEvent_t bev[3]{};     // batch march bracket
+    pcc::MarchLaunchInfo batch_launch{};
+    pcc::Server* server = nullptr;  // serving loop (serve.cpp), created by the first submit
+};
+
+struct pcc_solve {
+    pcc_ctx* ctx = nullptr;
+    pcc_solve_desc d{};
+    int nn = 0;      // Nnewton
+    int ngrid = 0;   // nl + nr + 1
+    int stages = 2;
+    double a[3][3]{}, b[3]{}, c[3]{};
+    double dm2c = 0.0;
+    std::vector<double> grid;
+    // device buffers
+    double* d_grid = nullptr;
+    double2* d_tw = nullptr;
+    double* d_in0 = nullptr;
+    double* d_out0 = nullptr;
+    double* d_J = nullptr;
+    double* d_yinit = nullptr;    // [2*(nn+1)][N]
+    double* d_yfinal = nullptr;   // [2*(nn+1)][N]
+    double* d_outc = nullptr;     // [nn+1][nn]
+    int* d_status = nullptr;      // [2*(nn+1)] march status
+    int* d_fail = nullptr;        // [2*(nn+1)]
+    int* d_cstatus = nullptr;     // [nn+1] epilogue status
+    int* d_counters_i = nullptr;  // [4] work counters
+    unsigned long long* d_counters = nullptr;  // [4] march counters
+    double* d_scratch = nullptr;
+    int scratch_ctas = 0;
+    int* d_item_side = nullptr;   // pcc_sweep
+    double* d_xs = nullptr;       // pcc_sweep / test entry points (x_in, x_out)
+    int* d_its = nullptr;
+    // device-resident Newton iteration (newton.cu)
+    pcc::NewtonDev* d_newton = nullptr;
+    double* d_in0old = nullptr;
+    double* d_rhs = nullptr;
+    double* d_dx = nullptr;
+    int* d_ipiv = nullptr;
+    int* d_info = nullptr;    // [2]: LU info, FP64 fallback flag
+    void* d_luw = nullptr;    // mixed-precision LU workspace
+    int* d_cancel = nullptr;  // nonzero: remaining sweeps of this solve are skipped
+    size_t footprint = 0;     // device bytes held by this solve
+    int h_newton = -1;        // host copy of the Newton state code (-1: no iteration begun)
+    // last asynchronous build
+    int pend_c0 = 0, pend_c1 = 0;
+    bool pending = false;
+    cudaEvent_t ev[5]{};
+    pcc::MarchLaunchInfo last_launch{};
+};
+
+
+namespace pcc {
+
+// Stops the serving loop of ctx, if one runs, and releases its solves.
+void server_shutdown(pcc_ctx* ctx);
+
+inline pcc_status fail(pcc_ctx* ctx, pcc_status s, const std::string& msg)
+{
+    if (ctx) ctx->last_error = msg;
+    return s;
+}
+
+}  // namespace pcc
+
+#define PCC_CUDA(ctx, call)                                                                          \
+    do {                                                                                             \
+        cudaError_t _e = (call);                                                                     \
+        if (_e != cudaSuccess) {                                                                     \
+            return pcc::fail((ctx), _e == cudaErrorMemoryAllocation ? PCC_ERR_OOM : PCC_ERR_CUDA,    \
+                             std::string(#call) + ": " + cudaGetErrorString(_e));                    \
+        }                                                                                            \
+    } while (0)

@@ -473,6 +473,65 @@ json NewtonSolver::run(json* benchmark_result)
     return resultDict;
 }
 
+std::vector<json> NewtonSolver::runBatched(const std::vector<NewtonSolver*>& solvers)
+{
+    std::vector<json> out(solvers.size());
+    std::vector<size_t> idx;
+    for (size_t k = 0; k < solvers.size(); ++k) {
+        if (solvers[k]->Converged)
+            out[k] = solvers[k]->run();  // one shoot to report the stored solution
+        else
+            idx.push_back(k);
+    }
+    if (idx.empty()) return out;
+    std::vector<pcc_solve*> handles;
+    std::vector<vec_real> x(idx.size());
+    std::vector<double*> xp;
+    for (size_t j = 0; j < idx.size(); ++j) {
+        NewtonSolver* a = solvers[idx[j]];
+        a->initGen.packSpectralFields(a->Up, a->psic, a->fc, a->in0);
+        a->in0[2 * a->Nnewton / 3 + 2] = a->Delta;
+        x[j] = a->in0;
+        handles.push_back(a->solve);
+        xp.push_back(x[j].data());
+    }
+    std::vector<pcc_newton_state> st(idx.size());
+    const pcc_precision prec = solvers[idx[0]]->linearPrecision;
+    check(pcc_newton_solve(device_context(), (int)idx.size(), handles.data(), xp.data(), prec, st.data(), nullptr),
+          "pcc_newton_solve");
+    std::string failures;
+    for (size_t j = 0; j < idx.size(); ++j) {
+        NewtonSolver* a = solvers[idx[j]];
+        const pcc_newton_state& s = st[j];
+        std::cout << "D = " << a->Dim << ": " << s.iterations << " Newton iterations, mismatch norm " << s.err << std::endl;
+        if (s.code == PCC_NEWTON_CONVERGED || s.code == PCC_NEWTON_STOPPED) {
+            // the result iterate (the last improving one when stopped) -> fields, as :306-321
+            vec_real z = x[j];
+            a->in0 = z;
+            a->Delta = z[2 * a->Nnewton / 3 + 2];
+            z[2 * a->Nnewton / 3 + 2] = 0.0;
+            a->initGen.unpackSpectralFields(z, a->Up, a->psic, a->fc);
+            a->Converged = true;
+            if (s.code == PCC_NEWTON_CONVERGED) {
+                std::cout << "The solution has converged!" << std::endl << std::endl;
+                a->writeFinalOutput((size_t)(s.iterations - 1), s.err);
+            } else {
+                std::cerr << "Mismatch increased - terminating Newton.\n";
+                a->writeFinalOutput((size_t)(s.iterations - 1), s.err_old);
+            }
+            out[idx[j]] = a->resultDict;
+        } else {
+            const char* what = s.code == PCC_NEWTON_MAX_ITER         ? "Newton method did not converge"
+                               : s.code == PCC_NEWTON_IRK_FAILED      ? "IRK iteration did not converge"
+                               : s.code == PCC_NEWTON_DELTA_MISMATCH ? "Delta mismatch between the sides"
+                                                                      : "singular Jacobian";
+            failures += std::string(failures.empty() ? "" : "; ") + what + " for dimension " + std::to_string(a->Dim);
+        }
+    }
+    if (!failures.empty()) throw pcc::Error(PCC_ERR_NEWTON_NO_CONVERGENCE, failures);
+    return out;
+}
+
 void NewtonSolver::writeFinalOutput(size_t newtonIts, real_t mismatchNorm)
 {
     resultDict["Ntau"] = Ntau;

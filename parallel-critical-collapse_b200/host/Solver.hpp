@@ -100,6 +100,14 @@ class NewtonSolver {
     json run(json* benchmark_result = nullptr);
     void writeFinalOutput(size_t newtonIts, real_t mismatchNorm);
 
+    /// run() for several solvers at once through the device-resident Newton
+    /// loop (pcc_newton_solve): every iteration's shoots of all solvers still
+    /// running share one batch launch, and the loop state (mismatch history,
+    /// divergence counter, last improving iterate) stays on the device.  The
+    /// result dictionaries are those run() writes; failures throw pcc::Error
+    /// after every solver has finished.
+    static std::vector<json> runBatched(const std::vector<NewtonSolver*>& solvers);
+
     /// Precision of the dense Newton solve: PCC_PREC_FP64 (dgesv semantics,
     /// the default) or PCC_PREC_MIXED ($PCC_LU_PRECISION=mixed).
     pcc_precision linearPrecision = PCC_PREC_FP64;

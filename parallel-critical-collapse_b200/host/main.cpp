@@ -1,29 +1,45 @@
-// main.cpp -- cc_b200: the reference's command line (src/main.cpp:19-235) for
-// single runs and benchmark mode, on the B200 engine.
+// main.cpp -- cc_b200: the reference's command line (src/main.cpp:19-378) on
+// the B200 engine.
 //
 //   cc_b200 [-s] -i data/simulation_4D_512.json [--ignore-converged]
 //   cc_b200 -b --benchmark-repetitions 3 -i ...
+//   cc_b200 -m -i suite.json [-r] [--ignore-converged]
+//   cc_b200 -m --suite up.json asc --suite down.json desc [--ignore-converged]
 //
 // Single run: the result dictionary is written back over the input file, as
 // the reference does (main.cpp:221-233).  Benchmark mode writes
 // benchmark_D=<D>_B200_1.json next to the input with the reference's keys
 // (Dim, Ntau, ..., Kind, per-repetition AssembleStep_k / NewtonStep_k /
-// OverallTime).  Suite mode (-m) is not part of this engine.
+// OverallTime).  Suite mode (-m) continues through the dimensions of a
+// multi-dimension file (-r: ascending, else descending), writing the file
+// after every dimension; --suite (repeatable, not in the reference) names
+// several such files with their own order, which then run in lockstep with
+// their Newton solves batched together.
 #include <cstring>
 
-#include "Solver.hpp"
+#include "Suite.hpp"
 
 int main(int argc, char** argv)
 {
-    bool benchmark = false, ignoreConverged = false;
+    bool benchmark = false, ignoreConverged = false, multiple = false, reversed = false;
+    std::vector<std::pair<std::string, bool>> suiteSpecs;  // --suite path asc|desc
     int reps = 3;
     std::string inputPath = "data/simulation_4D_512.json";
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         if (a == "-s" || a == "--single-run") {
         } else if (a == "-m" || a == "--multiple-run") {
-            std::cerr << "cc_b200: suite mode (-m) is not provided by this engine\n";
-            return 2;
+            multiple = true;
+        } else if (a == "-r" || a == "--reversed-order") {
+            reversed = true;
+        } else if (a == "--suite") {
+            if (i + 2 >= argc || (std::string(argv[i + 2]) != "asc" && std::string(argv[i + 2]) != "desc")) {
+                std::cerr << "--suite needs <path> asc|desc\n";
+                return 2;
+            }
+            suiteSpecs.emplace_back(argv[i + 1], std::string(argv[i + 2]) == "asc");
+            i += 2;
+            multiple = true;
         } else if (a == "--ignore-converged") {
             ignoreConverged = true;
         } else if (a == "-i" || a == "--input-path") {
@@ -41,6 +57,17 @@ int main(int argc, char** argv)
     }
     const std::filesystem::path dataPath = std::filesystem::path(inputPath).parent_path();
     try {
+        if (multiple) {
+            if (suiteSpecs.empty()) suiteSpecs.emplace_back(inputPath, reversed);
+            std::vector<SimulationSuite> suites;
+            std::vector<std::string> paths;
+            for (const auto& sp : suiteSpecs) {
+                suites.emplace_back(sp.first, sp.second, ignoreConverged);
+                paths.push_back(sp.first);
+            }
+            runSuites(suites, paths, ignoreConverged, std::filesystem::path(paths[0]).parent_path());
+            return 0;
+        }
         SimulationConfig config = SimulationConfig::loadFromJson(inputPath);
         if (ignoreConverged) config.Converged = false;
         if (benchmark) {

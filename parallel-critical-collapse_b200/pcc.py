@@ -34,7 +34,11 @@ EXPORTS = ["pcc_ctx_create", "pcc_ctx_destroy", "pcc_status_string", "pcc_last_e
            "pcc_solve_destroy", "pcc_solve_grid", "pcc_shoot", "pcc_jacobian", "pcc_jacobian_device",
            "pcc_solve_sync", "pcc_jacobian_columns", "pcc_lu_solve", "pcc_newton_step", "pcc_rhs_eval",
            "pcc_irk_step", "pcc_boundary_data", "pcc_sweep", "pcc_fp64_peak", "pcc_pack_fields",
-           "pcc_unpack_fields", "pcc_expansions", "pcc_solve_set_grid", "pcc_dft", "pcc_expansions_static"]
+           "pcc_unpack_fields", "pcc_expansions", "pcc_solve_set_grid", "pcc_dft", "pcc_expansions_static",
+           "pcc_jacobian_batch", "pcc_newton_begin", "pcc_newton_iterate", "pcc_newton_result",
+           "pcc_newton_solve"]
+
+NEWTON_CODES = ["RUNNING", "CONVERGED", "STOPPED", "MAX_ITER", "IRK_FAILED", "DELTA_MISMATCH", "SINGULAR"]
 
 
 class PccError(RuntimeError):
@@ -80,6 +84,18 @@ class RefineReport(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class NewtonState(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("code", ctypes.c_int), ("err", ctypes.c_double),
+                ("err_old", ctypes.c_double), ("fail_column", ctypes.c_int), ("fail_side", ctypes.c_int),
+                ("fail_grid_index", ctypes.c_int), ("lu_refinement_steps", ctypes.c_int),
+                ("lu_fell_back", ctypes.c_int)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["state"] = NEWTON_CODES[self.code] if 0 <= self.code < len(NEWTON_CODES) else str(self.code)
+        return d
+
+
 _lib = None
 
 
@@ -120,6 +136,12 @@ def load(path=None):
     L.pcc_solve_set_grid.argtypes = [vp, _D]
     L.pcc_dft.argtypes = [vp, ci, ci, ci, _D, _D]
     L.pcc_expansions_static.argtypes = [vp, ci, cd, cd, cd, cd, vp, vp, vp, vp, vp]
+    PP = ctypes.POINTER(vp)
+    L.pcc_jacobian_batch.argtypes = [vp, ci, PP, PP, PP, PP, ctypes.POINTER(Stats)]
+    L.pcc_newton_begin.argtypes = [vp, _D]
+    L.pcc_newton_iterate.argtypes = [vp, ci, PP, ci, ctypes.POINTER(NewtonState), ctypes.POINTER(Stats)]
+    L.pcc_newton_result.argtypes = [vp, _D, ctypes.POINTER(NewtonState)]
+    L.pcc_newton_solve.argtypes = [vp, ci, PP, PP, ci, ctypes.POINTER(NewtonState), ctypes.POINTER(Stats)]
     for name in EXPORTS:
         if name not in ("pcc_status_string", "pcc_last_error"):
             getattr(L, name).restype = ci
@@ -225,6 +247,40 @@ class Engine:
                                      out.ctypes.data_as(_D)))
         return out
 
+    @staticmethod
+    def _ptrs(items):
+        return (ctypes.c_void_p * len(items))(*[ctypes.c_void_p(x) for x in items])
+
+    def jacobian_batch(self, solves, in0s, out0s, stats=None):
+        """assembleJacobian for several solves in one batch launch -> list of J."""
+        ins = [_f64(a) for a in in0s]
+        outs = [_f64(a) for a in out0s]
+        Js = [np.zeros((a.size, a.size)) for a in ins]
+        st = stats if stats is not None else Stats()
+        self._check(self.lib.pcc_jacobian_batch(
+            self.ctx, len(solves), self._ptrs([s.h.value for s in solves]),
+            self._ptrs([a.ctypes.data for a in ins]), self._ptrs([a.ctypes.data for a in outs]),
+            self._ptrs([J.ctypes.data for J in Js]), ctypes.byref(st)))
+        return Js
+
+    def newton_iterate(self, solves, precision=PREC_FP64, stats=None):
+        """One device-resident Newton iteration of every running solve -> states."""
+        states = (NewtonState * len(solves))()
+        st = stats if stats is not None else Stats()
+        self._check(self.lib.pcc_newton_iterate(self.ctx, len(solves), self._ptrs([s.h.value for s in solves]),
+                                                precision, states, ctypes.byref(st)))
+        return [x.as_dict() for x in states]
+
+    def newton_solve(self, solves, in0s, precision=PREC_FP64, stats=None):
+        """NewtonSolver::run for several solves at once -> (results, states)."""
+        xs = [_f64(a).copy() for a in in0s]
+        states = (NewtonState * len(solves))()
+        st = stats if stats is not None else Stats()
+        self._check(self.lib.pcc_newton_solve(self.ctx, len(solves), self._ptrs([s.h.value for s in solves]),
+                                              self._ptrs([x.ctypes.data for x in xs]), precision, states,
+                                              ctypes.byref(st)))
+        return xs, [x.as_dict() for x in states]
+
     def fp64_peak_tflops(self):
         v = ctypes.c_double(0)
         self._check(self.lib.pcc_fp64_peak(self.ctx, ctypes.byref(v)))
@@ -312,6 +368,15 @@ class Solve:
         self.engine._check(self.lib.pcc_newton_step(self.h, _p(x), ctypes.byref(err), precision, ctypes.byref(st),
                                                     ctypes.byref(rep)))
         return x, err.value, st.as_dict(), rep.as_dict()
+
+    def newton_begin(self, in0):
+        self.engine._check(self.lib.pcc_newton_begin(self.h, _p(_f64(in0))))
+
+    def newton_result(self):
+        x = np.zeros(3 * self.desc.ntau // 4)
+        st = NewtonState()
+        self.engine._check(self.lib.pcc_newton_result(self.h, _p(x), ctypes.byref(st)))
+        return x, st.as_dict()
 
     def boundary_data(self, in0):
         in0 = _f64(in0)

@@ -45,6 +45,11 @@ def test_null_arguments_rejected_without_device():
     assert lib.pcc_lu_solve(None, 0, None, None, None, 0, None) == 1
     assert lib.pcc_rhs_eval(None, 128, 4.0, 1, None, None, None) == 1
     assert lib.pcc_ctx_destroy(None) == 1
+    assert lib.pcc_jacobian_batch(None, 1, None, None, None, None, None) == 1
+    assert lib.pcc_newton_begin(None, None) == 1
+    assert lib.pcc_newton_iterate(None, 1, None, 0, None, None) == 1
+    assert lib.pcc_newton_result(None, None, None) == 1
+    assert lib.pcc_newton_solve(None, 1, None, None, 0, None, None) == 1
 
 
 def test_struct_layouts_match_header(tmp_path):
@@ -56,7 +61,8 @@ def test_struct_layouts_match_header(tmp_path):
 
     if shutil.which("gcc") is None:
         pytest.skip("no C compiler")
-    structs = {"pcc_solve_desc": pcc.SolveDesc, "pcc_stats": pcc.Stats, "pcc_refine_report": pcc.RefineReport}
+    structs = {"pcc_solve_desc": pcc.SolveDesc, "pcc_stats": pcc.Stats, "pcc_refine_report": pcc.RefineReport,
+               "pcc_newton_state": pcc.NewtonState}
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pcc.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
