@@ -190,6 +190,56 @@ pcc_status pcc_newton_result(pcc_solve* s, double* in0_out, pcc_newton_state* st
 pcc_status pcc_newton_solve(pcc_ctx* ctx, int count, pcc_solve* const* solves, double* const* in0,
                             pcc_precision prec, pcc_newton_state* states, pcc_stats* stats);
 
+/* ---- serving: whole Newton solves submitted over time --------------------
+ * A request is one NewtonSolver::run of its own SimulationConfig.  A
+ * scheduler thread inside the library admits requests in arrival order while
+ * the device bytes of the admitted solves fit the HBM budget (and the cap on
+ * concurrent solves), keeps each solve's Newton state on the device, and
+ * batches the sweeps of all admitted solves as they become ready into shared
+ * persistent launches, so that requests arriving while others run overlap
+ * with them on the device.  Each result equals the one the same request gives
+ * alone.  Ntau 128..1024 with 2 IRK stages.  While serving runs, the context
+ * takes only pcc_submit / pcc_poll / pcc_wait / pcc_serve_stats, from any
+ * thread; results can be read until pcc_serve_stop. */
+typedef struct {
+    size_t hbm_budget_bytes; /* device bytes admitted solves may hold (0: 3/4 of the free memory at start) */
+    int max_active;          /* solves admitted at once (0: limited by the budget only) */
+} pcc_serve_opts;
+
+typedef struct {
+    pcc_solve_desc desc;     /* the request's SimulationConfig */
+    const double* in0;       /* Nnewton initial unknowns (Delta at 2N/3+2), copied by pcc_submit */
+    pcc_precision precision; /* of its Newton solves */
+} pcc_request;
+
+typedef struct {
+    int done;                /* 1 once the solve has ended; the fields below are then final */
+    pcc_status status;       /* PCC_OK (converged, or stopped by the divergence safeguard) or why it failed */
+    pcc_newton_state newton; /* how the Newton loop ended */
+    double ms_queued;        /* submit -> admission (host clock) */
+    double ms_latency;       /* submit -> result available */
+    size_t footprint_bytes;  /* device bytes the solve held */
+} pcc_result;
+
+typedef struct {
+    long long submitted, completed, launches, sweeps;
+    int active, waiting;
+    size_t bytes_in_use, budget_bytes;
+} pcc_serve_info;
+
+/* Starts the loop (pcc_submit starts it with defaults when needed). */
+pcc_status pcc_serve_start(pcc_ctx* ctx, const pcc_serve_opts* opts);
+/* Queues a request; ticket identifies it in pcc_poll / pcc_wait. */
+pcc_status pcc_submit(pcc_ctx* ctx, const pcc_request* req, uint64_t* ticket);
+/* Non-blocking: out->done tells whether the solve has ended; x_out (optional,
+ * Nnewton) receives the result iterate once it has. */
+pcc_status pcc_poll(pcc_ctx* ctx, uint64_t ticket, pcc_result* out, double* x_out);
+/* As pcc_poll, waiting up to timeout_s seconds for the solve to end. */
+pcc_status pcc_wait(pcc_ctx* ctx, uint64_t ticket, double timeout_s, pcc_result* out, double* x_out);
+pcc_status pcc_serve_stats(pcc_ctx* ctx, pcc_serve_info* out);
+/* Finishes every submitted request, then stops the loop and drops the results. */
+pcc_status pcc_serve_stop(pcc_ctx* ctx);
+
 /* ---- lower-level entry points (the reference's inner class methods) ---- */
 
 /* ODEStepper::computeDerivatives (ODEStepper.cpp:92-136) for `count` states:

@@ -22,7 +22,7 @@ using namespace pcc;
 
 cudaStream_t pcc_ctx_stream(pcc_ctx* ctx) { return ctx->stream; }
 int pcc_ctx_device(pcc_ctx* ctx) { return ctx->device; }
-void pcc_ctx_set_error(pcc_ctx* ctx, const char* msg) { ctx->last_error = msg; }
+void pcc_ctx_set_error(pcc_ctx* ctx, const char* msg) { fail(ctx, PCC_OK, msg); }
 
 namespace {
 
@@ -281,128 +281,34 @@ pcc_status collect(pcc_solve* s, int c0, int c1, pcc_stats* stats)
     if (result != PCC_OK) {
         char buf[160];
         std::snprintf(buf, sizeof buf, "%s at column %d side %d grid index %d", kStatusNames[result], fcol, fside, fidx);
-        ctx->last_error = buf;
+        fail(ctx, result, buf);
     }
     return result;
 }
 
-// Grows a device buffer and its pinned host staging buffer to `bytes`.
-pcc_status batch_tables(pcc_ctx* ctx, size_t bytes)
-{
-    if (ctx->d_batch_bytes < bytes) {
-        if (ctx->d_batch) cudaFree(ctx->d_batch);
-        ctx->d_batch = nullptr;
-        ctx->d_batch_bytes = 0;
-        PCC_CUDA(ctx, cudaMalloc(&ctx->d_batch, bytes));
-        ctx->d_batch_bytes = bytes;
-    }
-    if (ctx->h_batch_bytes < bytes) {
-        if (ctx->h_batch) cudaFreeHost(ctx->h_batch);
-        ctx->h_batch = nullptr;
-        ctx->h_batch_bytes = 0;
-        PCC_CUDA(ctx, cudaMallocHost(&ctx->h_batch, bytes));
-        ctx->h_batch_bytes = bytes;
-    }
-    for (auto& ev : ctx->bev)
-        if (!ev) PCC_CUDA(ctx, cudaEventCreate(&ev));
-    return PCC_OK;
-}
-
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-// Builds the item table of a batch march over columns [0, ncols[i]) of every
-// solve: Ntau classes in decreasing order, inside a class the longest sweeps
-// first (longest-processing-time order), ties by solve and item.
-void batch_items(const std::vector<pcc_solve*>& v, const std::vector<int>& ncols, BatchParams& B,
-                 std::vector<int2>& items)
-{
-    static const int kOrder[kBatchMaxClasses] = {1024, 512, 256, 128};
-    items.clear();
-    B.n_classes = 0;
-    for (int n : kOrder) {
-        std::vector<std::pair<int, int2>> cls;  // (steps, item)
-        for (size_t i = 0; i < v.size(); ++i) {
-            if (v[i]->d.ntau != n) continue;
-            for (int k = 0; k < 2 * ncols[i]; ++k)
-                cls.push_back({(k & 1) ? v[i]->d.nr : v[i]->d.nl, make_int2((int)i, k)});
-        }
-        if (cls.empty()) continue;
-        std::stable_sort(cls.begin(), cls.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-        B.cls_ntau[B.n_classes] = n;
-        B.cls_begin[B.n_classes] = (int)items.size();
-        for (auto& c : cls) items.push_back(c.second);
-        B.n_classes += 1;
-    }
-    B.cls_begin[B.n_classes] = (int)items.size();
-}
-
 // One persistent launch over the sweeps of columns [0, ncols[i]) of every
-// solve in v (all batch-supported, same stage count), on stream st.
+// solve in v, with the context's own tables.
 pcc_status enqueue_batch_march(pcc_ctx* ctx, const std::vector<pcc_solve*>& v, const std::vector<int>& ncols,
                                cudaStream_t st)
 {
-    BatchParams B{};
-    std::vector<int2> items;
-    batch_items(v, ncols, B, items);
-    const size_t o_solves = 0;
-    const size_t o_items = align_up(o_solves + v.size() * sizeof(BatchSolve), 16);
-    const size_t o_cls = align_up(o_items + items.size() * sizeof(int2), 16);
-    const size_t o_cnt = align_up(o_cls + kBatchMaxClasses * sizeof(int), 16);
-    const size_t bytes = o_cnt + 4 * sizeof(unsigned long long);
-    pcc_status r = batch_tables(ctx, bytes);
-    if (r != PCC_OK) return r;
-    char* h = static_cast<char*>(ctx->h_batch);
-    char* d = static_cast<char*>(ctx->d_batch);
-    auto* hs = reinterpret_cast<BatchSolve*>(h + o_solves);
-    for (size_t i = 0; i < v.size(); ++i) {
-        pcc_solve* s = v[i];
-        BatchSolve& b = hs[i];
-        b.grid = s->d_grid;
-        b.twN = s->d_tw;
-        b.yinit = s->d_yinit;
-        b.yfinal = s->d_yfinal;
-        b.status = s->d_status;
-        b.fail_index = s->d_fail;
-        b.cancel = s->d_cancel;
-        b.dim = s->d.dim;
-        b.dm2c = s->dm2c;
-        b.prec = s->d.prec_irk;
-        b.nl = s->d.nl;
-        b.nr = s->d.nr;
-        b.max_its = s->d.max_irk;
-        b.ntau = s->d.ntau;
-    }
-    std::memcpy(h + o_items, items.data(), items.size() * sizeof(int2));
-    std::memset(h + o_cls, 0, o_cnt - o_cls + 4 * sizeof(unsigned long long));
-    PCC_CUDA(ctx, cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
-    B.solves = reinterpret_cast<const BatchSolve*>(d + o_solves);
-    B.items = reinterpret_cast<const int2*>(d + o_items);
-    B.cls_counter = reinterpret_cast<int*>(d + o_cls);
-    B.counters = reinterpret_cast<unsigned long long*>(d + o_cnt);
-    ctx->batch_cnt_off = o_cnt;
-    const pcc_solve* s0 = v[0];
-    for (int i = 0; i < 3; ++i) {
-        B.b[i] = s0->b[i];
-        B.c[i] = s0->c[i];
-        for (int j = 0; j < 3; ++j) B.a[i][j] = s0->a[i][j];
-    }
-    PCC_CUDA(ctx, cudaEventRecord(ctx->bev[0], st));
-    PCC_CUDA(ctx, launch_march_batch(B, 0, st, &ctx->batch_launch));
-    PCC_CUDA(ctx, cudaEventRecord(ctx->bev[1], st));
-    return PCC_OK;
+    std::vector<BatchItem> items;
+    for (size_t i = 0; i < v.size(); ++i)
+        for (int k = 0; k < 2 * ncols[i]; ++k) items.push_back({v[i], k});
+    return batch_march_items(ctx, ctx->batch, items, st, 0);
 }
 
 // Reads the counters and timing of the last batch march (stream synchronised).
-void batch_stats(pcc_ctx* ctx, const std::vector<pcc_solve*>& v, const std::vector<int>& ncols, pcc_stats* stats)
+void batch_stats(pcc_ctx* ctx, const std::vector<int>& ncols, pcc_stats* stats)
 {
     if (!stats) return;
     std::memset(stats, 0, sizeof(*stats));
-    (void)v;
     unsigned long long cnt[4] = {0, 0, 0, 0};
-    cudaMemcpy(cnt, static_cast<char*>(ctx->d_batch) + ctx->batch_cnt_off, 3 * sizeof(unsigned long long),
+    cudaMemcpy(cnt, static_cast<char*>(ctx->batch.d) + ctx->batch.cnt_off, 3 * sizeof(unsigned long long),
                cudaMemcpyDeviceToHost);
     float ms = 0;
-    cudaEventElapsedTime(&ms, ctx->bev[0], ctx->bev[1]);
+    cudaEventElapsedTime(&ms, ctx->batch.ev[0], ctx->batch.ev[1]);
     stats->rhs_evals = (long long)cnt[0];
     stats->irk_iterations = (long long)cnt[1];
     stats->irk_steps = (long long)cnt[2];
@@ -413,7 +319,7 @@ void batch_stats(pcc_ctx* ctx, const std::vector<pcc_solve*>& v, const std::vect
     stats->ms_total = ms;
     stats->fail_column = -1;
     stats->fail_grid_index = -1;
-    stats->sweep_ctas = ctx->batch_launch.ctas;
+    stats->sweep_ctas = ctx->batch.info.ctas;
 }
 
 // Finds the first failing sweep or column of a solve's last shoots.
@@ -479,53 +385,22 @@ void newton_state_from_dev(const NewtonDev& nd, pcc_newton_state* out)
 
 }  // namespace
 
-extern "C" {
+// ------------------------------------------------ shared with the serving loop
+namespace pcc {
 
-const char* pcc_status_string(pcc_status s)
+// Device bytes of one solve's buffers (the allocations of solve_create).
+size_t solve_footprint(const pcc_solve_desc& d, int sms)
 {
-    const int i = (int)s;
-    return (i >= 0 && i < (int)(sizeof(kStatusNames) / sizeof(kStatusNames[0]))) ? kStatusNames[i] : "PCC_UNKNOWN";
+    const size_t n = d.ntau, nn = 3 * n / 4, cols = nn + 1, ngrid = (size_t)d.nl + d.nr + 1;
+    const size_t dbl = sizeof(double), in = sizeof(int);
+    return ngrid * dbl + n * sizeof(double2) + 2 * nn * dbl + nn * nn * dbl + 2 * (2 * cols * n * dbl) +
+           cols * nn * dbl + 2 * (2 * cols * in) + cols * in + 4 * in + 4 * sizeof(unsigned long long) +
+           (size_t)2 * sms * kBoundaryArrays * n * dbl + 2 * cols * in + 4 * cols * dbl + 2 * cols * in +
+           sizeof(NewtonDev) + 3 * nn * dbl + nn * in + 2 * in + lu_mixed_work_bytes((int)nn) + in;
 }
 
-const char* pcc_last_error(pcc_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
-
-pcc_status pcc_ctx_create(int device, const pcc_ctx_opts* opts, pcc_ctx** out)
-{
-    if (!out) return PCC_ERR_INVALID_ARG;
-    *out = nullptr;
-    if (opts && opts->reserved != 0) return PCC_ERR_INVALID_ARG;
-    int count = 0;
-    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return PCC_ERR_CUDA;
-    auto* ctx = new pcc_ctx;
-    ctx->device = device;
-    if (cudaSetDevice(device) != cudaSuccess ||
-        cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        delete ctx;
-        return PCC_ERR_CUDA;
-    }
-    *out = ctx;
-    return PCC_OK;
-}
-
-pcc_status pcc_ctx_destroy(pcc_ctx* ctx)
-{
-    if (!ctx) return PCC_ERR_INVALID_ARG;
-    cudaSetDevice(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
-    server_shutdown(ctx);
-    while (!ctx->solves.empty()) pcc_solve_destroy(ctx->solves.back());
-    if (ctx->lu_work) cudaFree(ctx->lu_work);
-    if (ctx->d_batch) cudaFree(ctx->d_batch);
-    if (ctx->h_batch) cudaFreeHost(ctx->h_batch);
-    for (auto& ev : ctx->bev)
-        if (ev) cudaEventDestroy(ev);
-    cudaStreamDestroy(ctx->stream);
-    delete ctx;
-    return PCC_OK;
-}
-
-pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve** out)
+pcc_status solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, cudaStream_t alloc_st, bool registered,
+                        pcc_solve** out)
 {
     if (!ctx || !out) return PCC_ERR_INVALID_ARG;
     *out = nullptr;
@@ -535,6 +410,7 @@ pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve*
     auto* s = new pcc_solve;
     s->ctx = ctx;
     s->d = *desc;
+    s->alloc_stream = alloc_st;
     s->nn = 3 * desc->ntau / 4;
     s->ngrid = desc->nl + desc->nr + 1;
     s->stages = tableau(desc->scheme, s->a, s->b, s->c);
@@ -543,12 +419,13 @@ pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve*
     const int n = desc->ntau, nn = s->nn, cols = nn + 1;
     s->scratch_ctas = 2 * ctx->sms;
     auto cleanup = [&](pcc_status st, const std::string& m) {
-        pcc_solve_destroy(s);
+        solve_release(s);
         return fail(ctx, st, m);
     };
 #define ALLOC(ptr, bytes)                                                                                    \
     do {                                                                                                     \
-        cudaError_t _e = cudaMalloc((void**)&(ptr), (bytes));                                                \
+        cudaError_t _e = alloc_st ? cudaMallocAsync((void**)&(ptr), (bytes), alloc_st)                       \
+                                  : cudaMalloc((void**)&(ptr), (bytes));                                     \
         if (_e != cudaSuccess) return cleanup(PCC_ERR_OOM, std::string("cudaMalloc ") + #ptr + ": " + cudaGetErrorString(_e)); \
         s->footprint += (bytes);                                                                             \
     } while (0)
@@ -578,16 +455,223 @@ pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve*
     ALLOC(s->d_luw, lu_mixed_work_bytes(nn));
     ALLOC(s->d_cancel, sizeof(int));
 #undef ALLOC
-    const std::vector<double2> tw = twiddles(n);
-    cudaError_t e = cudaMemcpy(s->d_tw, tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(s->d_grid, s->grid.data(), s->ngrid * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(s->d_cancel, 0, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(s->d_newton, 0, sizeof(NewtonDev));
+    cudaStream_t st = alloc_st ? alloc_st : ctx->stream;
+    s->tw_host = twiddles(n);
+    cudaError_t e = cudaMemcpyAsync(s->d_tw, s->tw_host.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->d_grid, s->grid.data(), s->ngrid * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_cancel, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_newton, 0, sizeof(NewtonDev), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the host tables may go once copied
     for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&s->ev[i]);
     if (e != cudaSuccess) return cleanup(PCC_ERR_CUDA, cudaGetErrorString(e));
-    ctx->solves.push_back(s);
+    if (registered) ctx->solves.push_back(s);
     *out = s;
     return PCC_OK;
+}
+
+void solve_release(pcc_solve* s)
+{
+    void* ptrs[] = {s->d_grid, s->d_tw, s->d_in0, s->d_out0, s->d_J, s->d_yinit, s->d_yfinal, s->d_outc,
+                    s->d_status, s->d_fail, s->d_cstatus, s->d_counters_i, s->d_counters, s->d_scratch,
+                    s->d_item_side, s->d_xs, s->d_its, s->d_newton, s->d_in0old, s->d_rhs, s->d_dx,
+                    s->d_ipiv, s->d_info, s->d_luw, s->d_cancel};
+    for (void* p : ptrs)
+        if (p) {
+            if (s->alloc_stream)
+                cudaFreeAsync(p, s->alloc_stream);  // stream-ordered: no device-wide synchronisation
+            else
+                cudaFree(p);
+        }
+    for (auto& ev : s->ev)
+        if (ev) cudaEventDestroy(ev);
+    delete s;
+}
+
+pcc_status newton_reset(pcc_solve* s, const double* in0_host, cudaStream_t st)
+{
+    pcc_ctx* ctx = s->ctx;
+    PCC_CUDA(ctx, cudaMemcpyAsync(s->d_in0, in0_host, s->nn * sizeof(double), cudaMemcpyHostToDevice, st));
+    PCC_CUDA(ctx, launch_newton_reset(s->d_newton, s->d_in0, s->d_in0old, s->nn, st));
+    PCC_CUDA(ctx, cudaMemsetAsync(s->d_cancel, 0, sizeof(int), st));
+    s->h_newton = kNewtonRunning;
+    return PCC_OK;
+}
+
+pcc_status newton_prologue(pcc_solve* s, cudaStream_t st) { return enqueue_prologue(s, 0, s->nn + 1, st); }
+
+pcc_status newton_tail(pcc_solve* s, pcc_precision prec, cudaStream_t st, int* lu_steps, int* lu_fallback)
+{
+    return enqueue_newton_tail(s, prec, st, lu_steps, lu_fallback);
+}
+
+pcc_status batch_tables_reserve(pcc_ctx* ctx, BatchTables& tab, size_t bytes)
+{
+    if (tab.d_bytes < bytes) {
+        if (tab.d) cudaFree(tab.d);
+        tab.d = nullptr;
+        tab.d_bytes = 0;
+        PCC_CUDA(ctx, cudaMalloc(&tab.d, bytes));
+        tab.d_bytes = bytes;
+    }
+    if (tab.h_bytes < bytes) {
+        if (tab.h) cudaFreeHost(tab.h);
+        tab.h = nullptr;
+        tab.h_bytes = 0;
+        PCC_CUDA(ctx, cudaMallocHost(&tab.h, bytes));
+        tab.h_bytes = bytes;
+    }
+    for (auto& ev : tab.ev)
+        if (!ev) PCC_CUDA(ctx, cudaEventCreate(&ev));
+    return PCC_OK;
+}
+
+void batch_tables_free(BatchTables& tab)
+{
+    if (tab.d) cudaFree(tab.d);
+    if (tab.h) cudaFreeHost(tab.h);
+    for (auto& ev : tab.ev)
+        if (ev) cudaEventDestroy(ev);
+    tab = BatchTables{};
+}
+
+// Item table: Ntau classes in decreasing order; inside a class the longest
+// sweeps first (longest-processing-time order), ties in list order.
+pcc_status batch_march_items(pcc_ctx* ctx, BatchTables& tab, const std::vector<BatchItem>& items,
+                             cudaStream_t st, int max_ctas)
+{
+    static const int kOrder[kBatchMaxClasses] = {1024, 512, 256, 128};
+    if (items.empty()) return PCC_OK;
+    std::vector<pcc_solve*> solves;
+    std::vector<int> sidx(items.size());
+    for (size_t i = 0; i < items.size(); ++i) {
+        pcc_solve* s = items[i].s;
+        if (!march_batch_supported(s->d.ntau, s->stages))
+            return fail(ctx, PCC_ERR_UNSUPPORTED, "batch: Ntau must be 128..1024 with 2 IRK stages");
+        auto it = std::find(solves.begin(), solves.end(), s);
+        sidx[i] = (int)(it - solves.begin());
+        if (it == solves.end()) solves.push_back(s);
+    }
+    BatchParams B{};
+    std::vector<int2> table;
+    table.reserve(items.size());
+    B.n_classes = 0;
+    for (int n : kOrder) {
+        std::vector<std::pair<int, size_t>> cls;  // (steps, index into items)
+        for (size_t i = 0; i < items.size(); ++i) {
+            const pcc_solve* s = items[i].s;
+            if (s->d.ntau == n) cls.push_back({(items[i].item & 1) ? s->d.nr : s->d.nl, i});
+        }
+        if (cls.empty()) continue;
+        std::stable_sort(cls.begin(), cls.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+        B.cls_ntau[B.n_classes] = n;
+        B.cls_begin[B.n_classes] = (int)table.size();
+        for (auto& c : cls) table.push_back(make_int2(sidx[c.second], items[c.second].item));
+        B.n_classes += 1;
+    }
+    B.cls_begin[B.n_classes] = (int)table.size();
+    const size_t o_items = align_up(solves.size() * sizeof(BatchSolve), 16);
+    const size_t o_cls = align_up(o_items + table.size() * sizeof(int2), 16);
+    const size_t o_cnt = align_up(o_cls + kBatchMaxClasses * sizeof(int), 16);
+    const size_t bytes = o_cnt + 4 * sizeof(unsigned long long);
+    pcc_status r = batch_tables_reserve(ctx, tab, bytes);
+    if (r != PCC_OK) return r;
+    char* h = static_cast<char*>(tab.h);
+    char* d = static_cast<char*>(tab.d);
+    auto* hs = reinterpret_cast<BatchSolve*>(h);
+    for (size_t i = 0; i < solves.size(); ++i) {
+        const pcc_solve* s = solves[i];
+        BatchSolve& b = hs[i];
+        b.grid = s->d_grid;
+        b.twN = s->d_tw;
+        b.yinit = s->d_yinit;
+        b.yfinal = s->d_yfinal;
+        b.status = s->d_status;
+        b.fail_index = s->d_fail;
+        b.cancel = s->d_cancel;
+        b.dim = s->d.dim;
+        b.dm2c = s->dm2c;
+        b.prec = s->d.prec_irk;
+        b.nl = s->d.nl;
+        b.nr = s->d.nr;
+        b.max_its = s->d.max_irk;
+        b.ntau = s->d.ntau;
+    }
+    std::memcpy(h + o_items, table.data(), table.size() * sizeof(int2));
+    std::memset(h + o_cls, 0, bytes - o_cls);
+    PCC_CUDA(ctx, cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
+    B.solves = reinterpret_cast<const BatchSolve*>(d);
+    B.items = reinterpret_cast<const int2*>(d + o_items);
+    B.cls_counter = reinterpret_cast<int*>(d + o_cls);
+    B.counters = reinterpret_cast<unsigned long long*>(d + o_cnt);
+    tab.cnt_off = o_cnt;
+    const pcc_solve* s0 = solves[0];
+    for (int i = 0; i < 3; ++i) {
+        B.b[i] = s0->b[i];
+        B.c[i] = s0->c[i];
+        for (int j = 0; j < 3; ++j) B.a[i][j] = s0->a[i][j];
+    }
+    PCC_CUDA(ctx, cudaEventRecord(tab.ev[0], st));
+    PCC_CUDA(ctx, launch_march_batch(B, max_ctas, st, &tab.info));
+    PCC_CUDA(ctx, cudaEventRecord(tab.ev[1], st));
+    return PCC_OK;
+}
+
+}  // namespace pcc
+
+extern "C" {
+
+const char* pcc_status_string(pcc_status s)
+{
+    const int i = (int)s;
+    return (i >= 0 && i < (int)(sizeof(kStatusNames) / sizeof(kStatusNames[0]))) ? kStatusNames[i] : "PCC_UNKNOWN";
+}
+
+const char* pcc_last_error(pcc_ctx* ctx)
+{
+    if (!ctx) return "null context";
+    static thread_local std::string copy;  // stable for the calling thread until its next call
+    std::lock_guard<std::mutex> lk(ctx->err_mu);
+    copy = ctx->last_error;
+    return copy.c_str();
+}
+
+pcc_status pcc_ctx_create(int device, const pcc_ctx_opts* opts, pcc_ctx** out)
+{
+    if (!out) return PCC_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (opts && opts->reserved != 0) return PCC_ERR_INVALID_ARG;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return PCC_ERR_CUDA;
+    auto* ctx = new pcc_ctx;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return PCC_ERR_CUDA;
+    }
+    *out = ctx;
+    return PCC_OK;
+}
+
+pcc_status pcc_ctx_destroy(pcc_ctx* ctx)
+{
+    if (!ctx) return PCC_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    server_shutdown(ctx);
+    while (!ctx->solves.empty()) pcc_solve_destroy(ctx->solves.back());
+    if (ctx->lu_work) cudaFree(ctx->lu_work);
+    batch_tables_free(ctx->batch);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return PCC_OK;
+}
+
+pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve** out)
+{
+    return solve_create(ctx, desc, nullptr, true, out);
 }
 
 pcc_status pcc_solve_destroy(pcc_solve* s)
@@ -597,15 +681,7 @@ pcc_status pcc_solve_destroy(pcc_solve* s)
     v.erase(std::remove(v.begin(), v.end(), s), v.end());
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
-    void* ptrs[] = {s->d_grid, s->d_tw, s->d_in0, s->d_out0, s->d_J, s->d_yinit, s->d_yfinal, s->d_outc,
-                    s->d_status, s->d_fail, s->d_cstatus, s->d_counters_i, s->d_counters, s->d_scratch,
-                    s->d_item_side, s->d_xs, s->d_its, s->d_newton, s->d_in0old, s->d_rhs, s->d_dx,
-                    s->d_ipiv, s->d_info, s->d_luw, s->d_cancel};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
-    for (auto& ev : s->ev)
-        if (ev) cudaEventDestroy(ev);
-    delete s;
+    solve_release(s);
     return PCC_OK;
 }
 
@@ -1109,7 +1185,7 @@ pcc_status pcc_jacobian_batch(pcc_ctx* ctx, int count, pcc_solve* const* solves,
                                       st));
     }
     PCC_CUDA(ctx, cudaStreamSynchronize(st));
-    batch_stats(ctx, v, ncols, stats);
+    batch_stats(ctx, ncols, stats);
     for (int i = 0; i < count; ++i) {
         int col, side, idx;
         solve_failure(v[i], ncols[i], &col, &side, &idx);
@@ -1192,7 +1268,7 @@ pcc_status pcc_newton_iterate(pcc_ctx* ctx, int count, pcc_solve* const* solves,
         if (stats && !batch.empty()) {
             std::vector<int> ncols;
             for (pcc_solve* s : batch) ncols.push_back(s->nn + 1);
-            batch_stats(ctx, batch, ncols, stats);
+            batch_stats(ctx, ncols, stats);
         }
         if (stats) {
             for (pcc_solve* s : single) {

@@ -1,6 +1,7 @@
 // pcc_objects.h -- the opaque objects of include/pcc.h and the error helpers
 // shared by the translation units that implement the C ABI.
 #pragma once
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -9,26 +10,32 @@
 
 namespace pcc {
 struct Server;
-}
+
+// Launch tables of one batch march: BatchSolve[], int2 items[], class
+// counters and march counters, in device memory with a pinned staging copy.
+struct BatchTables {
+    void* d = nullptr;
+    size_t d_bytes = 0;
+    void* h = nullptr;
+    size_t h_bytes = 0;
+    size_t cnt_off = 0;         // offset of the march counters
+    cudaEvent_t ev[2]{};        // bracket of the march launch
+    MarchLaunchInfo info{};
+};
+}  // namespace pcc
 
 struct pcc_ctx {
     int device = 0;
     int sms = 0;
     cudaStream_t stream = nullptr;
     std::string last_error;
+    std::mutex err_mu;  // guards last_error
     std::vector<pcc_solve*> solves;  // live solves; destroyed with the context
     // LU workspace (grown on demand)
     void* lu_work = nullptr;
     size_t lu_work_bytes = 0;
-    // batch launch tables (grown on demand): BatchSolve[], int2 items[], class counters, march counters
-    void* d_batch = nullptr;
-    size_t d_batch_bytes = 0;
-    void* h_batch = nullptr;  // pinned staging of the same layout
-    size_t h_batch_bytes = 0;
-    size_t batch_cnt_off = 0; // offset of the march counters in d_batch
-    cudaEvent_t bev[3]{};     // batch march bracket
-    pcc::MarchLaunchInfo batch_launch{};
-    pcc::Server* server = nullptr;  // serving loop (serve.cpp), created by the first submit
+    pcc::BatchTables batch;         // tables of the synchronous batch entry points
+    pcc::Server* server = nullptr;  // serving loop (serve.cu)
 };
 
 struct pcc_solve {
@@ -69,6 +76,8 @@ struct pcc_solve {
     void* d_luw = nullptr;    // mixed-precision LU workspace
     int* d_cancel = nullptr;  // nonzero: remaining sweeps of this solve are skipped
     size_t footprint = 0;     // device bytes held by this solve
+    cudaStream_t alloc_stream = nullptr;  // stream-ordered allocation (serving), else cudaMalloc
+    std::vector<double2> tw_host;         // twiddle table (source of the asynchronous upload)
     int h_newton = -1;        // host copy of the Newton state code (-1: no iteration begun)
     // last asynchronous build
     int pend_c0 = 0, pend_c1 = 0;
@@ -83,9 +92,32 @@ namespace pcc {
 // Stops the serving loop of ctx, if one runs, and releases its solves.
 void server_shutdown(pcc_ctx* ctx);
 
+// Building blocks shared with the serving loop (pcc_abi.cu).
+struct BatchItem {
+    pcc_solve* s;
+    int item;  // 2 column + side
+};
+// A solve whose buffers come from cudaMallocAsync on alloc_st (nullptr: cudaMalloc)
+// and which is not registered with its context.
+pcc_status solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, cudaStream_t alloc_st, bool registered,
+                        pcc_solve** out);
+void solve_release(pcc_solve* s);
+size_t solve_footprint(const pcc_solve_desc& d, int sms);
+pcc_status newton_reset(pcc_solve* s, const double* in0_host, cudaStream_t st);
+pcc_status newton_prologue(pcc_solve* s, cudaStream_t st);
+pcc_status newton_tail(pcc_solve* s, pcc_precision prec, cudaStream_t st, int* lu_steps, int* lu_fallback);
+// One persistent launch over an explicit list of sweeps (every solve batch-supported).
+pcc_status batch_march_items(pcc_ctx* ctx, BatchTables& tab, const std::vector<BatchItem>& items,
+                             cudaStream_t st, int max_ctas);
+pcc_status batch_tables_reserve(pcc_ctx* ctx, BatchTables& tab, size_t bytes);
+void batch_tables_free(BatchTables& tab);
+
 inline pcc_status fail(pcc_ctx* ctx, pcc_status s, const std::string& msg)
 {
-    if (ctx) ctx->last_error = msg;
+    if (ctx) {
+        std::lock_guard<std::mutex> lk(ctx->err_mu);  // the serving thread reports here too
+        ctx->last_error = msg;
+    }
     return s;
 }
 

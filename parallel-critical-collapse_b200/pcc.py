@@ -36,7 +36,8 @@ EXPORTS = ["pcc_ctx_create", "pcc_ctx_destroy", "pcc_status_string", "pcc_last_e
            "pcc_irk_step", "pcc_boundary_data", "pcc_sweep", "pcc_fp64_peak", "pcc_pack_fields",
            "pcc_unpack_fields", "pcc_expansions", "pcc_solve_set_grid", "pcc_dft", "pcc_expansions_static",
            "pcc_jacobian_batch", "pcc_newton_begin", "pcc_newton_iterate", "pcc_newton_result",
-           "pcc_newton_solve"]
+           "pcc_newton_solve", "pcc_serve_start", "pcc_submit", "pcc_poll", "pcc_wait", "pcc_serve_stats",
+           "pcc_serve_stop"]
 
 NEWTON_CODES = ["RUNNING", "CONVERGED", "STOPPED", "MAX_ITER", "IRK_FAILED", "DELTA_MISMATCH", "SINGULAR"]
 
@@ -96,6 +97,35 @@ class NewtonState(ctypes.Structure):
         return d
 
 
+class ServeOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_active", ctypes.c_int)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("desc", SolveDesc), ("in0", _D), ("precision", ctypes.c_int)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("done", ctypes.c_int), ("status", ctypes.c_int), ("newton", NewtonState),
+                ("ms_queued", ctypes.c_double), ("ms_latency", ctypes.c_double),
+                ("footprint_bytes", ctypes.c_size_t)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "newton"}
+        d["newton"] = self.newton.as_dict()
+        d["status_name"] = STATUS[self.status] if 0 <= self.status < len(STATUS) else str(self.status)
+        return d
+
+
+class ServeInfo(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("launches", ctypes.c_longlong), ("sweeps", ctypes.c_longlong), ("active", ctypes.c_int),
+                ("waiting", ctypes.c_int), ("bytes_in_use", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -142,6 +172,12 @@ def load(path=None):
     L.pcc_newton_iterate.argtypes = [vp, ci, PP, ci, ctypes.POINTER(NewtonState), ctypes.POINTER(Stats)]
     L.pcc_newton_result.argtypes = [vp, _D, ctypes.POINTER(NewtonState)]
     L.pcc_newton_solve.argtypes = [vp, ci, PP, PP, ci, ctypes.POINTER(NewtonState), ctypes.POINTER(Stats)]
+    L.pcc_serve_start.argtypes = [vp, ctypes.POINTER(ServeOpts)]
+    L.pcc_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]
+    L.pcc_poll.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(Result), _D]
+    L.pcc_wait.argtypes = [vp, ctypes.c_uint64, cd, ctypes.POINTER(Result), _D]
+    L.pcc_serve_stats.argtypes = [vp, ctypes.POINTER(ServeInfo)]
+    L.pcc_serve_stop.argtypes = [vp]
     for name in EXPORTS:
         if name not in ("pcc_status_string", "pcc_last_error"):
             getattr(L, name).restype = ci
@@ -280,6 +316,44 @@ class Engine:
                                               self._ptrs([x.ctypes.data for x in xs]), precision, states,
                                               ctypes.byref(st)))
         return xs, [x.as_dict() for x in states]
+
+    # -- serving ---------------------------------------------------------------
+    def serve_start(self, hbm_budget_bytes=0, max_active=0):
+        opts = ServeOpts(int(hbm_budget_bytes), int(max_active))
+        self._check(self.lib.pcc_serve_start(self.ctx, ctypes.byref(opts)))
+
+    def submit(self, cfg, in0, precision=PREC_FP64):
+        """Queues one Newton solve (a SimulationConfig dict or SolveDesc) -> ticket."""
+        desc = SolveDesc.from_config(cfg) if isinstance(cfg, dict) else cfg
+        x = _f64(in0)
+        req = Request(desc, _p(x), int(precision))
+        t = ctypes.c_uint64(0)
+        self._check(self.lib.pcc_submit(self.ctx, ctypes.byref(req), ctypes.byref(t)))
+        self._ticket_nn = getattr(self, "_ticket_nn", {})
+        self._ticket_nn[t.value] = 3 * desc.ntau // 4
+        return t.value
+
+    def _result(self, fn, ticket, *args):
+        r = Result()
+        x = np.zeros(self._ticket_nn[ticket])
+        self._check(fn(self.ctx, ctypes.c_uint64(ticket), *args, ctypes.byref(r), _p(x)))
+        d = r.as_dict()
+        return d, (x if r.done else None)
+
+    def poll(self, ticket):
+        """-> (result dict, x or None while running)."""
+        return self._result(self.lib.pcc_poll, ticket)
+
+    def wait(self, ticket, timeout_s=600.0):
+        return self._result(self.lib.pcc_wait, ticket, ctypes.c_double(timeout_s))
+
+    def serve_stats(self):
+        info = ServeInfo()
+        self._check(self.lib.pcc_serve_stats(self.ctx, ctypes.byref(info)))
+        return info.as_dict()
+
+    def serve_stop(self):
+        self._check(self.lib.pcc_serve_stop(self.ctx))
 
     def fp64_peak_tflops(self):
         v = ctypes.c_double(0)

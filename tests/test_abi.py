@@ -50,6 +50,12 @@ def test_null_arguments_rejected_without_device():
     assert lib.pcc_newton_iterate(None, 1, None, 0, None, None) == 1
     assert lib.pcc_newton_result(None, None, None) == 1
     assert lib.pcc_newton_solve(None, 1, None, None, 0, None, None) == 1
+    assert lib.pcc_serve_start(None, None) == 1
+    assert lib.pcc_submit(None, None, None) == 1
+    assert lib.pcc_poll(None, 1, None, None) == 1
+    assert lib.pcc_wait(None, 1, 0.0, None, None) == 1
+    assert lib.pcc_serve_stats(None, None) == 1
+    assert lib.pcc_serve_stop(None) == 1
 
 
 def test_struct_layouts_match_header(tmp_path):
@@ -62,7 +68,8 @@ def test_struct_layouts_match_header(tmp_path):
     if shutil.which("gcc") is None:
         pytest.skip("no C compiler")
     structs = {"pcc_solve_desc": pcc.SolveDesc, "pcc_stats": pcc.Stats, "pcc_refine_report": pcc.RefineReport,
-               "pcc_newton_state": pcc.NewtonState}
+               "pcc_newton_state": pcc.NewtonState, "pcc_serve_opts": pcc.ServeOpts, "pcc_request": pcc.Request,
+               "pcc_result": pcc.Result, "pcc_serve_info": pcc.ServeInfo}
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pcc.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

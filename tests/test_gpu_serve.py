@@ -1,0 +1,110 @@
+"""Serving: whole Newton solves submitted over time (pcc_submit / pcc_poll /
+pcc_wait), admitted by device-memory footprint, their sweeps batched into
+shared launches as they become ready.
+
+The property that matters for continuous batching: a request's result is the
+same alone and in a mix with requests of other sizes that arrive while it
+runs (bit for bit here, since every sweep and every per-solve kernel does the
+same arithmetic wherever it runs)."""
+import time
+
+import numpy as np
+import pytest
+
+from conftest import load_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _cfg(d, **over):
+    c = dict(d["cfg"])
+    c.update(over)
+    return c
+
+
+def _islot(x):
+    return 2 * x.size // 3 + 2
+
+
+def test_serve_same_alone_and_in_mix(engine):
+    c1, c2 = load_case("c1_newton"), load_case("c2_fixture")
+    cfg1 = _cfg(c1, PrecisionNewton=1e-12, MaxIterNewton=12)
+    engine.serve_start()
+    try:
+        t = engine.submit(cfg1, c1["in0"])
+        alone, x_alone = engine.wait(t)
+        assert alone["done"] == 1 and alone["status"] == 0, alone
+        assert alone["newton"]["state"] == "CONVERGED"
+        ref = c1["x_star"]
+        i = _islot(ref)
+        assert abs(x_alone[i] / ref[i] - 1) < 1e-10
+
+        # the mix: a larger solve first, then the same request twice, staggered
+        t_big = engine.submit(_cfg(c2, PrecisionNewton=1e-30, MaxIterNewton=2), c2["in0"])
+        time.sleep(0.05)
+        t_a = engine.submit(cfg1, c1["in0"])
+        time.sleep(0.02)
+        t_b = engine.submit(cfg1, c1["in0"])
+        ra, xa = engine.wait(t_a)
+        rb, xb = engine.wait(t_b)
+        rbig, _ = engine.wait(t_big)
+        assert np.array_equal(xa, x_alone) and np.array_equal(xb, x_alone)
+        assert ra["newton"]["iterations"] == alone["newton"]["iterations"]
+        assert ra["newton"]["err"] == alone["newton"]["err"]
+        assert rbig["newton"]["state"] == "MAX_ITER" and rbig["newton"]["iterations"] == 2
+        assert rbig["status"] == 10  # PCC_ERR_NEWTON_NO_CONVERGENCE, as the reference's exit
+        st = engine.serve_stats()
+        assert st["completed"] == 4 and st["launches"] >= 1 and st["sweeps"] > 0
+    finally:
+        engine.serve_stop()
+
+
+def test_serve_admission_by_memory_budget(engine):
+    c1 = load_case("c1_fixture")
+    cfg = _cfg(c1, PrecisionNewton=1e-30, MaxIterNewton=2)
+    engine.serve_start()
+    t = engine.submit(cfg, c1["in0"])
+    r0, x0 = engine.wait(t)
+    fp = r0["footprint_bytes"]
+    engine.serve_stop()
+    assert fp > 0
+    # room for one such solve at a time: the others wait for its memory
+    engine.serve_start(hbm_budget_bytes=int(fp * 1.5))
+    try:
+        ts = [engine.submit(cfg, c1["in0"]) for _ in range(3)]
+        peak = 0
+        while True:
+            st = engine.serve_stats()
+            peak = max(peak, st["bytes_in_use"])
+            if st["completed"] == 3:
+                break
+            time.sleep(0.005)
+        res = [engine.wait(t) for t in ts]
+        assert peak <= int(fp * 1.5)
+        for r, x in res:
+            assert r["done"] == 1 and np.array_equal(x, x0)
+        q = sorted(r["ms_queued"] for r, _ in res)
+        assert q[2] > q[0]  # the last one waited for memory
+    finally:
+        engine.serve_stop()
+
+
+def test_serve_rejects_solve_larger_than_budget(engine):
+    c1 = load_case("c1_fixture")
+    engine.serve_start(hbm_budget_bytes=1 << 20)
+    try:
+        r, x = engine.wait(engine.submit(_cfg(c1), c1["in0"]))
+        assert r["done"] == 1 and r["status"] == 3  # PCC_ERR_OOM
+    finally:
+        engine.serve_stop()
+
+
+def test_serve_reports_irk_failure(engine):
+    c1 = load_case("c1_fixture")
+    engine.serve_start()
+    try:
+        r, x = engine.wait(engine.submit(_cfg(c1, MaxIterIRK=1), c1["in0"]))
+        assert r["done"] == 1 and r["status"] == 4 and r["newton"]["state"] == "IRK_FAILED"
+        assert np.array_equal(x, c1["in0"])
+    finally:
+        engine.serve_stop()
