@@ -44,25 +44,55 @@ def f_rhs(n):
 
 def workload(seed, amp):
     """C3 config and seeded free data.  Free data: the reference's near-solution
-    (data/simulation_4D_1024.json, packed) plus, per field, amp * |c_lead| *
-    N(0,1) * exp(-k/8) on the coefficient of mode k (Delta unchanged)."""
+    (data/simulation_4D_1024.json, packed) plus perturb()'s seeded noise."""
     d = np.load(FIXTURE)
     cfg = json.loads(str(d["config"]))
-    in0 = d["in0"].copy()
-    nn = in0.size
-    third = nn // 3
-    rng = np.random.default_rng(seed)
+    return cfg, perturb(d["in0"], np.random.default_rng(seed), amp)
+
+
+def perturb(z, rng, amp):
+    """The free-data perturbation of workload(): per field, amp * |c_lead| *
+    N(0,1) * exp(-k/8) on the coefficient of mode k (Delta and the shared
+    cosine slot unchanged)."""
+    z = np.array(z, dtype=np.float64)
+    third = z.size // 3
     islot = 2 * third + 2
     for f in range(3):
-        blk = in0[f * third:(f + 1) * third]
-        modes = np.arange(third) // 2 * 2 + (1 if f < 2 else 0)  # odd fields: modes 1,3,..; even: 0,2,..
+        blk = z[f * third:(f + 1) * third]
+        modes = np.arange(third) // 2 * 2 + (1 if f < 2 else 0)
         lead = np.max(np.abs(blk[:2]))
         noise = amp * lead * rng.standard_normal(third) * np.exp(-modes / 8.0)
         if f == 2:
-            noise[islot - 2 * third] = 0.0  # Delta
-            noise[1] = 0.0                  # the shared cosine of mode Ntau/4 (packSpectralFields :710)
-        in0[f * third:(f + 1) * third] = blk + noise
-    return cfg, in0
+            noise[islot - 2 * third] = 0.0
+            noise[1] = 0.0
+        z[f * third:(f + 1) * third] = blk + noise
+    return z
+
+
+SEEDS = REPO / "bench_data" / "dscan_seeds_128.npz"
+
+# Fewest spatial points at which the reference's IRK fixed-point iteration
+# converges on this problem, per Ntau (checked on the compiled reference: at
+# Ntau = 1024 the converged fixture fails with 4000 and 6000 points, at the
+# right boundary and mid-grid).  The workloads draw points from [min, 8000].
+MIN_POINTS = {128: 2000, 256: 2000, 512: 4000, 1024: 8000}
+
+
+def seed_request(eng, seeds, dim, ntau, points):
+    """SimulationConfig and initial unknowns for dimension `dim`: the converged
+    continuation solution at the nearest tabulated D (Ntau 128, 1000+1000
+    points, bench_data/make_dscan_seeds.py), spectrally resampled to Ntau
+    (create_simulation_data.py double) on NLeft = NRight = points/2."""
+    i = int(np.argmin(np.abs(seeds["D"] - dim)))
+    cfg = json.loads(str(seeds["config"]))
+    cfg.update({"Dim": float(seeds["D"][i]), "Ntau": int(ntau), "NLeft": int(points) // 2,
+                "NRight": int(points) // 2, "EpsNewton": 1e-7 if ntau <= 256 else 1e-8})
+    fields = np.array([seeds["Up"][i], seeds["psic"][i], seeds["fc"][i]])
+    if ntau != fields.shape[1]:
+        fields = eng.resample(fields, ntau)
+    z = eng.pack(ntau, fields[0], fields[1], fields[2])
+    z[2 * z.size // 3 + 2] = seeds["delta"][i]
+    return cfg, z
 
 
 class Clocks:
@@ -195,6 +225,138 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+def newton_compare(eng, cfg, in0, out0, J):
+    """C3 Newton steps: the batched form (base shoot and all 768 columns in one
+    persistent launch, device-side Newton update) with the mixed-precision and
+    the FP64 solve, against the plain FP64 GPU form (one march launch per
+    shoot, 2 sweeps each, FP64 LU), timed on a column sample and extrapolated."""
+    import pcc
+
+    s = eng.solve(dict(cfg, PrecisionNewton=1e-30, MaxIterNewton=1000))
+    nn = s.nn
+    out = {"workload": "C3 (Ntau 1024, 4000+4000 points), one Newton iteration from the bench's seeded data"}
+    for name, prec in [("batched_mixed", pcc.PREC_MIXED), ("batched_fp64", pcc.PREC_FP64)]:
+        s.newton_begin(in0)
+        t = time.perf_counter()
+        st = eng.newton_iterate([s], precision=prec)[0]
+        out[f"ms_{name}"] = (time.perf_counter() - t) * 1e3
+        if prec == pcc.PREC_MIXED:
+            out["mixed_lu_refinement_steps"] = st["lu_refinement_steps"]
+            out["mixed_lu_fell_back_to_fp64"] = st["lu_fell_back"]
+    sample = 8
+    t = time.perf_counter()
+    for c in range(sample):
+        s.jacobian_columns(in0, out0, c, c + 1)
+    per_col = (time.perf_counter() - t) / sample
+    b = -np.asarray(out0)
+    t = time.perf_counter()
+    x64, _ = eng.lu_solve(J, b, precision=pcc.PREC_FP64)
+    lu_ms = (time.perf_counter() - t) * 1e3
+    xm, rep = eng.lu_solve(J, b, precision=pcc.PREC_MIXED)
+    x_lapack = np.linalg.solve(J, b)  # LAPACK dgesv (numpy)
+    out["ms_plain_fp64"] = per_col * (nn + 1) * 1e3 + lu_ms
+    out["plain_form"] = (f"one march launch per shoot (base + {nn} columns); {sample} columns timed, "
+                         f"extrapolated; FP64 LU {lu_ms:.1f} ms")
+    out["speedup_batched_mixed_vs_plain_fp64"] = out["ms_plain_fp64"] / out["ms_batched_mixed"]
+    out["speedup_batched_mixed_vs_batched_fp64"] = out["ms_batched_fp64"] / out["ms_batched_mixed"]
+    out["mixed_dx_rel_err_vs_fp64"] = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))
+    out["mixed_dx_rel_err_vs_lapack_dgesv"] = float(np.linalg.norm(xm - x_lapack) / np.linalg.norm(x_lapack))
+    out["fp64_dx_rel_err_vs_lapack_dgesv"] = float(np.linalg.norm(x64 - x_lapack) / np.linalg.norm(x_lapack))
+    s.close()
+    return out
+
+
+def run_dscan(eng, args):
+    """C4: 16 solves, D = 3.25, 3.35, .., 4.75, Ntau drawn from {128, 256, 512,
+    1024} and points from {2000, 4000, 6000, 8000} (seeded; at least
+    MIN_POINTS[Ntau]), seeded free data, one Newton iteration of all 16 in one
+    batch launch (mixed-precision solve)."""
+    import pcc
+
+    if not SEEDS.exists():
+        return {"unavailable": "bench_data/dscan_seeds_128.npz missing (bench_data/make_dscan_seeds.py)"}
+    seeds = np.load(SEEDS)
+    rng = np.random.default_rng(args.seed + 4)
+    dims = 3.25 + 0.1 * np.arange(16)
+    ns = rng.choice([128, 256, 512, 1024], 16)
+    pts = [int(rng.choice([p for p in (2000, 4000, 6000, 8000) if p >= MIN_POINTS[int(n)]])) for n in ns]
+    solves, xs, rejects = [], [], []
+    for d, n, p in zip(dims, ns, pts):
+        for attempt in range(4):
+            cfg, z = seed_request(eng, seeds, d, int(n), int(p))
+            z = perturb(z, rng, args.dscan_amp)
+            s = eng.solve(dict(cfg, PrecisionNewton=1e-30, MaxIterNewton=1000))
+            try:
+                s.shoot(z)  # the base shoot must converge (else re-draw, logged)
+                break
+            except pcc.PccError as e:
+                rejects.append({"D": float(d), "ntau": int(n), "points": int(p), "why": e.name})
+                s.close()
+                s = None
+        if s is not None:
+            solves.append(s)
+            xs.append(z)
+    for s, z in zip(solves, xs):  # warm-up iteration
+        s.newton_begin(z)
+    eng.newton_iterate(solves, precision=pcc.PREC_MIXED)
+    for s, z in zip(solves, xs):
+        s.newton_begin(z)
+    st = pcc.Stats()
+    t = time.perf_counter()
+    states = eng.newton_iterate(solves, precision=pcc.PREC_MIXED, stats=st)
+    wall = time.perf_counter() - t
+    out = {"solves": len(solves), "rejected_draws": rejects,
+           "ntau": [int(s.ntau) for s in solves], "points": [int(s.desc.nl + s.desc.nr) for s in solves],
+           "dims": [float(s.desc.dim) for s in solves], "wall_s": wall,
+           "jacobian_builds_per_s": len(solves) / wall, "ms_batch_march": st.ms_sweep,
+           "rhs_evals": st.rhs_evals, "sweeps": int(st.shoots) * 2,
+           "states": [x["state"] for x in states], "free_data_amp": args.dscan_amp,
+           "lu": "mixed (FP32 LU + FP64 refinement)"}
+    for s in solves:
+        s.close()
+    return out
+
+
+def run_serving(eng, args, rate, n_req):
+    """C5: a seeded Poisson stream of whole Newton solves, D ~ U[3.25, 4.75] (on
+    the 0.01 grid of the seed table), Ntau from {128, 256, 512, 1024}, points
+    ~ U[MIN_POINTS[Ntau], 8000]; latency = submit -> result (host clock)."""
+    if not SEEDS.exists():
+        return {"unavailable": "bench_data/dscan_seeds_128.npz missing (bench_data/make_dscan_seeds.py)"}
+    seeds = np.load(SEEDS)
+    rng = np.random.default_rng(args.seed + 5)
+    reqs = []
+    for _ in range(n_req):
+        d = rng.uniform(3.25, 4.75)
+        n = int(rng.choice([128, 256, 512, 1024]))
+        p = 2 * int(rng.integers(MIN_POINTS[n] // 2, 4001))
+        cfg, z = seed_request(eng, seeds, d, n, p)
+        cfg.update({"PrecisionNewton": 1e-10, "MaxIterNewton": 10})
+        reqs.append((cfg, z))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    eng.serve_start()
+    t0 = time.perf_counter()
+    tickets = []
+    for (cfg, z), a in zip(reqs, arrivals):
+        dt = t0 + a - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        tickets.append(eng.submit(cfg, z))
+    res = [eng.wait(t, 3600.0)[0] for t in tickets]
+    span = time.perf_counter() - t0
+    info = eng.serve_stats()
+    eng.serve_stop()
+    lat = np.array([r["ms_latency"] for r in res])
+    return {"rate_per_s": rate, "requests": n_req, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+            "throughput_solves_per_s": n_req / span, "span_s": span,
+            "converged": int(sum(r["newton"]["state"] == "CONVERGED" for r in res)),
+            "statuses": [r["status_name"] for r in res],
+            "iterations": [r["newton"]["iterations"] for r in res],
+            "ntau": [c["Ntau"] for c, _ in reqs], "launches": info["launches"], "sweeps": info["sweeps"],
+            "precision": "fp64", "newton_tolerance": 1e-10}
+
+
 def run_engine(args, world, rank, local):
     import torch
 
@@ -282,6 +444,10 @@ def run_engine(args, world, rank, local):
                 "flops_per_launch": flops_per_launch, "rhs_evals_per_launch": rhs / args.steps,
                 "flop_convention": "7*5*N*log2(N) + 100*N per RHS evaluation (reference algorithm)"}
 
+    newton = newton_compare(eng, cfg, in0, out0, h_J.numpy().copy()) if not args.quick else None
+    dscan = run_dscan(eng, args) if not args.quick else None
+    serving = run_serving(eng, args, args.rate, args.requests) if not args.quick else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         ref_so = REPO / "oracle" / "_ref" / "libpcc_ref.so"
@@ -301,7 +467,7 @@ def run_engine(args, world, rank, local):
                            "parallelism": f"{world} independent solves, one per GPU",
                            "sweep_ctas": st_e.sweep_ctas, "wall_s": wall},
                 "clocks": clk, "e2e": e2e, "gpu_launches": 4 * args.steps, "roofline": roofline,
-                "cpu_baseline": cpu}
+                "cpu_baseline": cpu, "newton_step": newton, "dscan16": dscan, "serving": serving}
         print(json.dumps(line))
     solve.close()
     eng.close()
@@ -316,6 +482,10 @@ def main():
     ap.add_argument("--seed", type=int, default=1024)
     ap.add_argument("--amp", type=float, default=0.1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--quick", action="store_true", help="only the Jacobian build line (no Newton/C4/C5 sections)")
+    ap.add_argument("--rate", type=float, default=4.0, help="C5 Poisson arrival rate (requests/s)")
+    ap.add_argument("--requests", type=int, default=16, help="C5 requests")
+    ap.add_argument("--dscan-amp", type=float, default=0.01, help="C4 free-data perturbation amplitude")
     ap.add_argument("--columns", type=int, default=0,
                     help="profiling aid: build only the first C columns (not a benchmark line)")
     args = ap.parse_args()

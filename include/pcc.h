@@ -111,6 +111,16 @@ pcc_status pcc_solve_grid(pcc_solve* s, double* grid_out /* nl+nr+1 */);
 /* NewtonSolver::shoot (NewtonSolver.cpp:403-423): in0 -> out0, host arrays. */
 pcc_status pcc_shoot(pcc_solve* s, const double* in0, double* out0, pcc_stats* stats);
 
+/* pcc_shoot with the reference's Debug field export (ShootingSolver.cpp:
+ * 85-97, 128-138): the state at the start of every step from grid index i
+ * with i % debug_nx == 0, and at the ends of each sweep (left sweep ascending,
+ * then right sweep descending, the reference's order), converted to A =
+ * 1/sqrt(IA2), U, V, f on Ntau points.  *count gets the number of snapshots;
+ * grid_idx[count] and fields[count][4][Ntau] are filled when count <=
+ * max_snaps (else PCC_ERR_INVALID_ARG and nothing runs). */
+pcc_status pcc_shoot_debug(pcc_solve* s, const double* in0, double* out0, int debug_nx, int max_snaps, int* count,
+                           int* grid_idx, double* fields, pcc_stats* stats);
+
 /* NewtonSolver::assembleJacobian (NewtonSolver.cpp:615-702): all Nnewton
  * columns in one persistent launch; host arrays, J row-major. */
 pcc_status pcc_jacobian(pcc_solve* s, const double* in0, const double* out0, double* J, pcc_stats* stats);
@@ -286,6 +296,12 @@ pcc_status pcc_expansions(pcc_ctx* ctx, int ntau, double dim, double delta, doub
 pcc_status pcc_expansions_static(pcc_ctx* ctx, int ntau, double dim, double delta, double x_l, double x_r,
                                  const double* d_fc, const double* d_psic, const double* d_up, double* d_y_left,
                                  double* d_y_right);
+
+/* Spectral refinement of periodic fields for convergence studies (the
+ * reference's scripts/create_simulation_data.py:37-58, double): count fields
+ * of ntau_in samples (row-major) -> count x ntau_out samples, doubling
+ * log2(ntau_out/ntau_in) times; powers of two, 4 <= ntau_in <= ntau_out <= 4096. */
+pcc_status pcc_resample_fields(pcc_ctx* ctx, int ntau_in, int ntau_out, int count, const double* in, double* out);
 
 /* Replaces the solve's x-grid (NewtonSolver::generateGrid output) by grid,
  * NLeft + NRight + 1 points, as ShootingSolver::shoot accepts any gridX. */

@@ -43,7 +43,7 @@ def _units():
         units.append((CSRC / "march.cu", OBJ / f"march_n{n}.o", [f"-DPCC_MARCH_N={n}"]))
     units.append((CSRC / "march.cu", OBJ / "march_dispatch.o", ["-DPCC_MARCH_DISPATCH"]))
     units.append((CSRC / "march.cu", OBJ / "march_batch.o", ["-DPCC_MARCH_BATCH"]))
-    for name in ["boundary", "lu", "newton", "pcc_abi", "serve", "static_scratch"]:
+    for name in ["boundary", "lu", "newton", "pcc_abi", "resample", "serve", "static_scratch"]:
         units.append((CSRC / f"{name}.cu", OBJ / f"{name}.o", []))
     return units
 

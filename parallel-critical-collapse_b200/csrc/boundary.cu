@@ -507,6 +507,73 @@ __global__ void __launch_bounds__(256) dft_kernel(int n, int sign, const double2
     for (int j = threadIdx.x; j < n; j += blockDim.x) y[j] = B.sa[j];
 }
 
+// The Debug field export of ShootingSolver::integrateToMatchPoint
+// (ShootingSolver.cpp:85-97, 128-138): a state snapshot at x ->
+// InitialConditionGenerator::StateVectorToFields (InitialConditionGenerator.cpp:
+// 791-884: doubleModes, the phase fix, the inverse transform and the split,
+// the IA2 constraint solve) -> A = sqrt(1/IA2), U, V, f.  One CTA per snapshot.
+__global__ void __launch_bounds__(256) debug_fields_kernel(int ntau, double dim, double dm2c, int count,
+                                                          const double* __restrict__ states,
+                                                          const double* __restrict__ xs, double* fields,
+                                                          double* scratch, const double2* __restrict__ tw)
+{
+    extern __shared__ double2 sh[];
+    Blk B;
+    B.n = ntau;
+    B.tw = tw;
+    B.sa = sh;
+    B.sb = sh + ntau;
+    B.scr = scratch + (size_t)blockIdx.x * kBoundaryArrays * ntau;
+    const int h = ntau / 2;
+    for (int k = blockIdx.x; k < count; k += gridDim.x) {
+        const double2* y = reinterpret_cast<const double2*>(states + (size_t)k * ntau);
+        const double delta = y[2].x;
+        const double x = xs[k];
+        for (int j = threadIdx.x; j < ntau; j += blockDim.x) B.sa[j] = double_modes_at(y, h, j);
+        B.sync();
+        if (threadIdx.x == 0) B.sa[2].x = -B.sa[ntau - 2].x;  // Re c[2] = -Re c[N-2]
+        B.sync();
+        B.backward();
+        double *U = B.arr(0), *V = B.arr(1), *F = B.arr(2), *k1 = B.arr(3), *k2 = B.arr(4), *ia2 = B.arr(5);
+        for (int j = threadIdx.x; j < h; j += blockDim.x) {
+            const double2 a = B.sa[j], b = B.sa[j + h];
+            const double u = 0.5 * (a.x - b.x), v = 0.5 * (a.y - b.y), f = 0.5 * (a.y + b.y);
+            U[j] = u;
+            V[j] = v;
+            F[j] = f;
+            U[j + h] = -u;
+            V[j + h] = -v;
+            F[j + h] = f;
+        }
+        B.sync();
+        for (int j = threadIdx.x; j < ntau; j += blockDim.x) {
+            k1[j] = -(((x + F[j]) * U[j] * U[j] + (x - F[j]) * V[j] * V[j]) * dm2c / (8.0 * x) + (dim - 3.0));
+            k2[j] = dim - 3.0;
+        }
+        B.sync();
+        B.solve_inhom(k1, k2, ia2, delta, B.arr(6));
+        double* o = fields + (size_t)k * 4 * ntau;
+        for (int j = threadIdx.x; j < ntau; j += blockDim.x) {
+            o[j] = sqrt(1.0 / ia2[j]);
+            o[ntau + j] = U[j];
+            o[2 * ntau + j] = V[j];
+            o[3 * ntau + j] = F[j];
+        }
+        B.sync();
+    }
+}
+
+cudaError_t launch_debug_fields(int ntau, double dim, double dm2c, int count, const double* states, const double* xs,
+                                double* fields, double* scratch, int ctas, const double2* tw, cudaStream_t st)
+{
+    const size_t smem = 2 * (size_t)ntau * sizeof(double2);
+    cudaError_t e = cudaFuncSetAttribute(debug_fields_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    debug_fields_kernel<<<ctas < count ? ctas : count, 256, smem, st>>>(ntau, dim, dm2c, count, states, xs, fields,
+                                                                        scratch, tw);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_dft(int n, int count, int sign, const double2* tw, const double2* in, double2* out,
                        cudaStream_t st)
 {

@@ -63,6 +63,8 @@ struct MarchParams {
     int* fail_index;   // [item]: grid index the failing step started from
     int* its_out;      // [item] (mode 2), may be null
     unsigned long long* counters;  // [0] RHS evaluations [1] IRK iterations [2] steps
+    const int* snap_slot;          // optional, per grid index: snapshot slot of the state there, or -1
+    double* snap;                  // [slot][N] states at the start of the steps snap_slot marks
 };
 
 template <int N, int S>
@@ -595,6 +597,8 @@ struct ParamScalars {
     __device__ __forceinline__ int* status(int item) const { return P.status + item; }
     __device__ __forceinline__ int* fail_index(int item) const { return P.fail_index + item; }
     __device__ __forceinline__ int* its_out(int item) const { return P.its_out ? P.its_out + item : nullptr; }
+    __device__ __forceinline__ int snap_slot(int gi) const { return P.snap_slot ? P.snap_slot[gi] : -1; }
+    __device__ __forceinline__ double* snap_base() const { return P.snap; }
 };
 
 // ------------------------------------------------------------ one sweep
@@ -639,6 +643,21 @@ __device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S>& sl, d
         }
         const double dx = xout - xin;
         const double xs = xin + dx * sc.c(s);
+        if (mode == 0) {
+            // the state at the start of this step, for the Debug field export
+            // (ShootingSolver.cpp:85-97, 128-138)
+            const int slot = sc.snap_slot(gi);
+            if (slot >= 0 && active && s == 0) {
+                double* o = sc.snap_base() + (size_t)slot * N;
+#pragma unroll
+                for (int sg = 0; sg < 8; ++sg) {
+                    const int m = slot_mode<N>(sg, t);
+                    const double2 y = ys[sg * TG + t];
+                    o[2 * m] = y.x;
+                    o[2 * m + 1] = y.y;
+                }
+            }
+        }
 
         bool converged = false;
         int its_reached = 0;
@@ -850,6 +869,8 @@ struct SmemScalars {
     __device__ __forceinline__ int* status(int) const { return p->status; }
     __device__ __forceinline__ int* fail_index(int) const { return p->fail_index; }
     __device__ __forceinline__ int* its_out(int) const { return nullptr; }
+    __device__ __forceinline__ int snap_slot(int) const { return -1; }
+    __device__ __forceinline__ double* snap_base() const { return nullptr; }
 };
 
 template <int S>

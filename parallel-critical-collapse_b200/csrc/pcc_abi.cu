@@ -728,6 +728,72 @@ pcc_status pcc_shoot(pcc_solve* s, const double* in0, double* out0, pcc_stats* s
     return pcc_jacobian_columns(s, in0, nullptr, s->nn, s->nn + 1, out0, stats);
 }
 
+pcc_status pcc_shoot_debug(pcc_solve* s, const double* in0, double* out0, int debug_nx, int max_snaps, int* count,
+                           int* grid_idx, double* fields, pcc_stats* stats)
+{
+    if (!s || !in0 || !out0 || !count || debug_nx < 1 || max_snaps < 0) return PCC_ERR_INVALID_ARG;
+    pcc_ctx* ctx = s->ctx;
+    const int nl = s->d.nl, nr = s->d.nr, n = s->d.ntau, nn = s->nn;
+    // snapshot grid indices in the reference's export order
+    std::vector<int> idx;
+    for (int i = 0; i < nl; ++i)
+        if (i % debug_nx == 0 || i == nl - 1) idx.push_back(i);
+    for (int i = nl + nr; i > nl; --i)
+        if (i % debug_nx == 0 || i == nl + 1 || i == nl + nr) idx.push_back(i);
+    *count = (int)idx.size();
+    if ((int)idx.size() > max_snaps || !grid_idx || !fields)
+        return fail(ctx, PCC_ERR_INVALID_ARG, "pcc_shoot_debug: max_snaps is below the snapshot count (see *count)");
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const int k = (int)idx.size();
+    std::vector<int> slot(s->ngrid, -1);
+    std::vector<double> xs(k);
+    for (int j = 0; j < k; ++j) {
+        slot[idx[j]] = j;
+        xs[j] = s->grid[idx[j]];
+    }
+    char* buf = nullptr;
+    const size_t bytes = s->ngrid * sizeof(int) + 16 + (size_t)k * n * sizeof(double) * 5 + k * sizeof(double);
+    PCC_CUDA(ctx, cudaMalloc(&buf, bytes));
+    int* d_slot = reinterpret_cast<int*>(buf);
+    double* d_snap = reinterpret_cast<double*>(buf + align_up(s->ngrid * sizeof(int), 16));
+    double* d_fields = d_snap + (size_t)k * n;
+    double* d_xs = d_fields + (size_t)k * 4 * n;
+    auto run = [&]() -> pcc_status {
+        PCC_CUDA(ctx, cudaMemcpyAsync(d_slot, slot.data(), s->ngrid * sizeof(int), cudaMemcpyHostToDevice, st));
+        PCC_CUDA(ctx, cudaMemcpyAsync(d_xs, xs.data(), k * sizeof(double), cudaMemcpyHostToDevice, st));
+        PCC_CUDA(ctx, cudaMemcpyAsync(s->d_in0, in0, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+        PCC_CUDA(ctx, cudaEventRecord(s->ev[0], st));
+        pcc_status r = enqueue_prologue(s, nn, nn + 1, st);
+        if (r != PCC_OK) return r;
+        PCC_CUDA(ctx, cudaEventRecord(s->ev[1], st));
+        MarchParams P = march_params(s);
+        P.n_items = 2;
+        P.mode = 0;
+        P.yinit = s->d_yinit;
+        P.yfinal = s->d_yfinal;
+        P.work_counter = s->d_counters_i + 1;
+        P.snap_slot = d_slot;
+        P.snap = d_snap;
+        PCC_CUDA(ctx, launch_march(n, s->stages, P, 0, st, &s->last_launch));
+        PCC_CUDA(ctx, cudaEventRecord(s->ev[2], st));
+        r = enqueue_epilogue(s, nn, nn + 1, false, nullptr, st);
+        if (r != PCC_OK) return r;
+        PCC_CUDA(ctx, cudaEventRecord(s->ev[3], st));
+        if (k > 0)
+            PCC_CUDA(ctx, launch_debug_fields(n, s->d.dim, s->dm2c, k, d_snap, d_xs, d_fields, s->d_scratch,
+                                              s->scratch_ctas, s->d_tw, st));
+        PCC_CUDA(ctx, cudaMemcpyAsync(out0, s->d_outc, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+        PCC_CUDA(ctx, cudaMemcpyAsync(fields, d_fields, (size_t)k * 4 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        return collect(s, nn, nn + 1, stats);
+    };
+    const pcc_status r = run();
+    cudaStreamSynchronize(st);
+    cudaFree(buf);
+    for (int j = 0; j < k; ++j) grid_idx[j] = idx[j];
+    return r;
+}
+
 pcc_status pcc_jacobian_device(pcc_solve* s, const double* d_in0, const double* d_out0, double* d_J)
 {
     if (!s || !d_in0 || !d_out0 || !d_J) return PCC_ERR_INVALID_ARG;
@@ -1138,6 +1204,45 @@ pcc_status pcc_dft(pcc_ctx* ctx, int n, int count, int sign, const double* in, d
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, d + (size_t)count * n, bytes, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(d);
+    if (e != cudaSuccess) return fail(ctx, PCC_ERR_CUDA, cudaGetErrorString(e));
+    return PCC_OK;
+}
+
+pcc_status pcc_resample_fields(pcc_ctx* ctx, int ntau_in, int ntau_out, int count, const double* in, double* out)
+{
+    if (!ctx || !in || !out || count < 1) return PCC_ERR_INVALID_ARG;
+    auto pow2 = [](int n) { return n >= 4 && (n & (n - 1)) == 0; };
+    if (!pow2(ntau_in) || !pow2(ntau_out) || ntau_out < ntau_in || ntau_out > 4096)
+        return fail(ctx, PCC_ERR_INVALID_ARG, "resample: powers of two with 4 <= Ntau_in <= Ntau_out <= 4096");
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t m = (size_t)count * ntau_out;
+    std::vector<double2> tws;
+    std::vector<size_t> tw_off;
+    for (int n = ntau_in; n <= ntau_out; n *= 2) {
+        tw_off.push_back(tws.size());
+        const std::vector<double2> t = twiddles(n);
+        tws.insert(tws.end(), t.begin(), t.end());
+    }
+    char* buf = nullptr;
+    const size_t bytes = 2 * m * sizeof(double2) + 2 * m * sizeof(double) + tws.size() * sizeof(double2);
+    PCC_CUDA(ctx, cudaMalloc(&buf, bytes));
+    double2* w0 = reinterpret_cast<double2*>(buf);
+    double2* w1 = w0 + m;
+    double* x0 = reinterpret_cast<double*>(w1 + m);
+    double* x1 = x0 + m;
+    double2* dtw = reinterpret_cast<double2*>(x1 + m);
+    cudaError_t e = cudaMemcpyAsync(dtw, tws.data(), tws.size() * sizeof(double2), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(x0, in, (size_t)count * ntau_in * sizeof(double), cudaMemcpyHostToDevice, st);
+    double* cur = x0;
+    double* nxt = x1;
+    for (int n = ntau_in, k = 0; n < ntau_out && e == cudaSuccess; n *= 2, ++k) {
+        e = launch_double_fields(n, count, cur, nxt, dtw + tw_off[k], dtw + tw_off[k + 1], w0, w1, st);
+        std::swap(cur, nxt);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, cur, m * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(buf);
     if (e != cudaSuccess) return fail(ctx, PCC_ERR_CUDA, cudaGetErrorString(e));
     return PCC_OK;
 }

@@ -16,6 +16,14 @@ cudaError_t launch_expansions(int ntau, double dim, double delta, double xl, dou
                               double* yr, cudaStream_t st);
 cudaError_t launch_dft(int n, int count, int sign, const double2* tw, const double2* in, double2* out,
                        cudaStream_t st);
+// One spectral doubling of count periodic fields of n samples (resample.cu):
+// out has count x 2n values; tw_n / tw_2n are exp(+2 pi i k/m) tables and
+// w0, w1 work arrays of count x 2n complex values.
+cudaError_t launch_double_fields(int n, int count, const double* in, double* out, const double2* tw_n,
+                                 const double2* tw_2n, double2* w0, double2* w1, cudaStream_t st);
+// Debug field export: count state snapshots at xs -> fields [count][4][ntau] = A, U, V, f.
+cudaError_t launch_debug_fields(int ntau, double dim, double dm2c, int count, const double* states, const double* xs,
+                                double* fields, double* scratch, int ctas, const double2* tw, cudaStream_t st);
 cudaError_t launch_fd(const double* outc, const double* out0, double* J, int nn, int c0, int ncols, double eps,
                       cudaStream_t st);
 

@@ -1,6 +1,8 @@
 // Solver.cpp -- the host classes of Solver.hpp over the C ABI (include/pcc.h).
 #include "Solver.hpp"
 
+#include <iomanip>
+
 #include <chrono>
 #include <cstring>
 #include <mutex>
@@ -299,7 +301,7 @@ void ShootingSolver::shoot(vec_complex& YLeft, vec_complex& YRight, const vec_re
     if (iLeft != 0 || iRight + 1 != gridX.size() || iMid <= iLeft || iMid >= iRight)
         throw pcc::Error(PCC_ERR_UNSUPPORTED, "shoot expects iLeft = 0 < iMid < iRight = gridX.size() - 1");
     if (config && config->Debug && fieldVals)
-        std::cerr << "[pcc] Debug field snapshots are not produced by the device march\n";
+        std::cerr << "[pcc] Debug field snapshots come from NewtonSolver::run (pcc_shoot_debug), not this call\n";
     const size_t nl = iMid - iLeft, nr = iRight - iMid;
     if (!solve || nl != cachedL || nr != cachedR) {
         if (solve) pcc_solve_destroy(solve);
@@ -381,6 +383,43 @@ void NewtonSolver::shoot(vec_real& inputVec, vec_real& outputVec)
     check(pcc_shoot(solve, inputVec.data(), outputVec.data(), &st), "pcc_shoot");
 }
 
+// every n-th element and the last one (common.cpp:201-215)
+static vec_real every_nth_element(const vec_real& a, size_t n)
+{
+    vec_real out;
+    for (size_t i = 0; i < a.size(); ++i)
+        if (i % n == 0 || i == a.size() - 1) out.push_back(a[i]);
+    return out;
+}
+
+void NewtonSolver::shootDebug(vec_real& inputVec, vec_real& outputVec, json& fieldVals)
+{
+    Delta = inputVec[2 * Nnewton / 3 + 2];
+    vec_real z = inputVec;
+    z[2 * Nnewton / 3 + 2] = 0.0;
+    initGen.unpackSpectralFields(z, Up, psic, fc);
+    outputVec.resize(Nnewton);
+    int count = 0;
+    pcc_shoot_debug(solve, inputVec.data(), outputVec.data(), (int)config.DebugNx, 0, &count, nullptr, nullptr,
+                    nullptr);  // counts the snapshots
+    std::vector<int> idx(count);
+    vec_real fields((size_t)count * 4 * Ntau);
+    pcc_stats st{};
+    check(pcc_shoot_debug(solve, inputVec.data(), outputVec.data(), (int)config.DebugNx, count, &count, idx.data(),
+                          fields.data(), &st),
+          "pcc_shoot_debug");
+    vec_real grid(NLeft + NRight + 1);
+    check(pcc_solve_grid(solve, grid.data()), "pcc_solve_grid");
+    static const char* names[4] = {"A", "U", "V", "f"};
+    for (int k = 0; k < count; ++k) {
+        const std::string key = std::to_string(grid[idx[k]]);
+        for (int q = 0; q < 4; ++q) {
+            const real_t* f = &fields[((size_t)k * 4 + q) * Ntau];
+            fieldVals[key][names[q]] = every_nth_element(vec_real(f, f + Ntau), config.DebugNtau);
+        }
+    }
+}
+
 void NewtonSolver::assembleJacobian(const vec_real& baseInput, const vec_real& baseOutput, mat_real& jacobian)
 {
     std::cout << "Starting to assemble Jacobian: " << std::endl << std::endl;
@@ -420,7 +459,15 @@ json NewtonSolver::run(json* benchmark_result)
             if (benchmark) newtonStart = clk::now();
             std::cout << "Newton iteration: " << its + 1 << std::endl;
             errOld = err;
-            shoot(in0, out0);
+            if (config.Debug) {
+                // the base shoot with the field export (NewtonSolver.cpp:287-295)
+                json fieldVals;
+                shootDebug(in0, out0, fieldVals);
+                const auto fieldPath = baseFolder / ("fields_" + std::to_string(Dim) + "_" + std::to_string(its) + ".json");
+                SimulationConfig::saveToJson(fieldPath.string(), fieldVals);
+            } else {
+                shoot(in0, out0);
+            }
             err = computeL2Norm(out0);
             std::cout << "Mismatch norm: " << err << std::endl;
             if (err < TolNewton) {
@@ -442,6 +489,18 @@ json NewtonSolver::run(json* benchmark_result)
             mat_real J;
             if (benchmark) assembleStart = clk::now();
             assembleJacobian(in0, out0, J);
+            if (config.Debug) {
+                // NewtonSolver.cpp:337-341 and OutputWriter::writeMatrix
+                const auto jacPath =
+                    baseFolder / ("jacobian_" + std::to_string(Dim) + "_" + std::to_string(its + 1) + ".csv");
+                std::ofstream outfile(jacPath);
+                if (!outfile) throw std::runtime_error("Could not open file for writing: " + jacPath.string());
+                outfile << std::setprecision(16);
+                for (size_t i = 0; i < J.size(); ++i) {
+                    for (size_t j = 0; j + 1 < J[i].size(); ++j) outfile << J[i][j] << ", ";
+                    outfile << J[i][J[i].size() - 1] << std::endl;
+                }
+            }
             if (benchmark)
                 (*benchmark_result)["AssembleStep_" + std::to_string(its + 1)] =
                     static_cast<double>((clk::now() - assembleStart).count()) / 1e9;
@@ -473,9 +532,11 @@ json NewtonSolver::run(json* benchmark_result)
     return resultDict;
 }
 
-std::vector<json> NewtonSolver::runBatched(const std::vector<NewtonSolver*>& solvers)
+std::vector<json> NewtonSolver::runBatched(const std::vector<NewtonSolver*>& solvers,
+                                           std::vector<std::string>* errors)
 {
     std::vector<json> out(solvers.size());
+    if (errors) errors->assign(solvers.size(), std::string());
     std::vector<size_t> idx;
     for (size_t k = 0; k < solvers.size(); ++k) {
         if (solvers[k]->Converged)
@@ -525,10 +586,12 @@ std::vector<json> NewtonSolver::runBatched(const std::vector<NewtonSolver*>& sol
                                : s.code == PCC_NEWTON_IRK_FAILED      ? "IRK iteration did not converge"
                                : s.code == PCC_NEWTON_DELTA_MISMATCH ? "Delta mismatch between the sides"
                                                                       : "singular Jacobian";
-            failures += std::string(failures.empty() ? "" : "; ") + what + " for dimension " + std::to_string(a->Dim);
+            const std::string msg = std::string(what) + " for dimension " + std::to_string(a->Dim);
+            if (errors) (*errors)[idx[j]] = msg;
+            failures += std::string(failures.empty() ? "" : "; ") + msg;
         }
     }
-    if (!failures.empty()) throw pcc::Error(PCC_ERR_NEWTON_NO_CONVERGENCE, failures);
+    if (!failures.empty() && !errors) throw pcc::Error(PCC_ERR_NEWTON_NO_CONVERGENCE, failures);
     return out;
 }
 

@@ -104,9 +104,11 @@ class NewtonSolver {
     /// loop (pcc_newton_solve): every iteration's shoots of all solvers still
     /// running share one batch launch, and the loop state (mismatch history,
     /// divergence counter, last improving iterate) stays on the device.  The
-    /// result dictionaries are those run() writes; failures throw pcc::Error
-    /// after every solver has finished.
-    static std::vector<json> runBatched(const std::vector<NewtonSolver*>& solvers);
+    /// result dictionaries are those run() writes.  Failures throw pcc::Error
+    /// after every solver has finished, unless `errors` is given: then
+    /// errors[k] describes solver k's failure ("" when it converged).
+    static std::vector<json> runBatched(const std::vector<NewtonSolver*>& solvers,
+                                        std::vector<std::string>* errors = nullptr);
 
     /// Precision of the dense Newton solve: PCC_PREC_FP64 (dgesv semantics,
     /// the default) or PCC_PREC_MIXED ($PCC_LU_PRECISION=mixed).
@@ -126,6 +128,8 @@ class NewtonSolver {
     pcc_solve* solve = nullptr;
 
     void shoot(vec_real& inputVec, vec_real& outputVec);
+    /// shoot with the Debug field export (ShootingSolver.cpp:85-97, 128-138)
+    void shootDebug(vec_real& inputVec, vec_real& outputVec, json& fieldVals);
     void assembleJacobian(const vec_real& baseInput, const vec_real& baseOutput, mat_real& jacobian);
     void solveLinearSystem(const mat_real& A, vec_real& rhs, vec_real& dx);
     real_t computeL2Norm(const vec_real& vc);

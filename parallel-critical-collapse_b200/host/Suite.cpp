@@ -132,9 +132,11 @@ void seedSuiteEntry(const SimulationSuite& suite, size_t i, SimulationConfig& co
     config.psic = psic;
 }
 
-void runSuites(std::vector<SimulationSuite>& suites, const std::vector<std::string>& paths, bool ignoreConverged,
-               const std::filesystem::path& dataPath)
+std::string runSuites(std::vector<SimulationSuite>& suites, const std::vector<std::string>& paths,
+                      bool ignoreConverged, const std::filesystem::path& dataPath)
 {
+    std::string failures;
+    std::vector<bool> stopped(suites.size(), false);
     size_t rounds = 0;
     for (const auto& s : suites) rounds = std::max(rounds, s.simulationDims.size());
     for (size_t k = 0; k < suites.size(); ++k)
@@ -145,24 +147,39 @@ void runSuites(std::vector<SimulationSuite>& suites, const std::vector<std::stri
         std::vector<size_t> owner;
         for (size_t k = 0; k < suites.size(); ++k) {
             SimulationSuite& suite = suites[k];
-            if (i >= suite.simulationDims.size()) continue;
+            if (stopped[k] || i >= suite.simulationDims.size()) continue;
             const std::string& simDim = suite.simulationDims[i];
             std::cout << "Simulation " << i + 1 << "/" << suite.simulationDims.size() << ":\n"
                       << "Starting simulation for D=" << simDim << ".\n\n";
             SimulationConfig config = suite.generateSimulation(simDim);
-            seedSuiteEntry(suite, i, config);
+            try {
+                seedSuiteEntry(suite, i, config);
+            } catch (const std::exception& e) {
+                stopped[k] = true;
+                failures += std::string(failures.empty() ? "" : "; ") + e.what();
+                continue;
+            }
             if (ignoreConverged) config.Converged = false;
             solvers.push_back(std::make_unique<NewtonSolver>(config, dataPath));
             owner.push_back(k);
         }
         std::vector<NewtonSolver*> raw;
         for (auto& s : solvers) raw.push_back(s.get());
-        const std::vector<json> results = NewtonSolver::runBatched(raw);
+        if (raw.empty()) break;
+        std::vector<std::string> errs;
+        const std::vector<json> results = NewtonSolver::runBatched(raw, &errs);
         for (size_t j = 0; j < raw.size(); ++j) {
             SimulationSuite& suite = suites[owner[j]];
+            if (!errs[j].empty()) {
+                std::cerr << "ERROR: " << errs[j] << std::endl;
+                stopped[owner[j]] = true;
+                failures += std::string(failures.empty() ? "" : "; ") + errs[j];
+                continue;
+            }
             suite.multiInputDict[suite.simulationDims[i]] = results[j];
             std::cout << "Result stored in file: " << paths[owner[j]] << "\n\n";
             SimulationConfig::saveToJson(paths[owner[j]], suite.multiInputDict);
         }
     }
+    return failures;
 }

@@ -43,6 +43,8 @@ void seedSuiteEntry(const SimulationSuite& suite, size_t i, SimulationConfig& co
 
 /// Runs the suites in lockstep (see the file comment).  After every round each
 /// suite's dictionary is written back to its path, as the reference writes
-/// its file after every dimension.
-void runSuites(std::vector<SimulationSuite>& suites, const std::vector<std::string>& paths, bool ignoreConverged,
-               const std::filesystem::path& dataPath);
+/// its file after every dimension.  A suite whose dimension fails stops there
+/// (the reference exits; here the other suites go on) and the failure is
+/// returned; the result is empty when every suite finished.
+std::string runSuites(std::vector<SimulationSuite>& suites, const std::vector<std::string>& paths,
+                      bool ignoreConverged, const std::filesystem::path& dataPath);

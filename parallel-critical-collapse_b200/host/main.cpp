@@ -65,7 +65,12 @@ int main(int argc, char** argv)
                 suites.emplace_back(sp.first, sp.second, ignoreConverged);
                 paths.push_back(sp.first);
             }
-            runSuites(suites, paths, ignoreConverged, std::filesystem::path(paths[0]).parent_path());
+            const std::string failed = runSuites(suites, paths, ignoreConverged,
+                                                 std::filesystem::path(paths[0]).parent_path());
+            if (!failed.empty()) {
+                std::cerr << "ERROR: " << failed << std::endl;
+                return 1;
+            }
             return 0;
         }
         SimulationConfig config = SimulationConfig::loadFromJson(inputPath);

@@ -37,7 +37,7 @@ EXPORTS = ["pcc_ctx_create", "pcc_ctx_destroy", "pcc_status_string", "pcc_last_e
            "pcc_unpack_fields", "pcc_expansions", "pcc_solve_set_grid", "pcc_dft", "pcc_expansions_static",
            "pcc_jacobian_batch", "pcc_newton_begin", "pcc_newton_iterate", "pcc_newton_result",
            "pcc_newton_solve", "pcc_serve_start", "pcc_submit", "pcc_poll", "pcc_wait", "pcc_serve_stats",
-           "pcc_serve_stop"]
+           "pcc_serve_stop", "pcc_resample_fields", "pcc_shoot_debug"]
 
 NEWTON_CODES = ["RUNNING", "CONVERGED", "STOPPED", "MAX_ITER", "IRK_FAILED", "DELTA_MISMATCH", "SINGULAR"]
 
@@ -178,6 +178,8 @@ def load(path=None):
     L.pcc_wait.argtypes = [vp, ctypes.c_uint64, cd, ctypes.POINTER(Result), _D]
     L.pcc_serve_stats.argtypes = [vp, ctypes.POINTER(ServeInfo)]
     L.pcc_serve_stop.argtypes = [vp]
+    L.pcc_resample_fields.argtypes = [vp, ci, ci, ci, _D, _D]
+    L.pcc_shoot_debug.argtypes = [vp, _D, _D, ci, ci, _I, _I, _D, ctypes.POINTER(Stats)]
     for name in EXPORTS:
         if name not in ("pcc_status_string", "pcc_last_error"):
             getattr(L, name).restype = ci
@@ -317,6 +319,26 @@ class Engine:
                                               ctypes.byref(st)))
         return xs, [x.as_dict() for x in states]
 
+    def resample(self, fields, ntau_out):
+        """create_simulation_data.py double(), repeated: rows of Ntau samples -> ntau_out samples."""
+        x = _f64(np.atleast_2d(fields))
+        out = np.zeros((x.shape[0], ntau_out))
+        self._check(self.lib.pcc_resample_fields(self.ctx, x.shape[1], ntau_out, x.shape[0], _p(x), _p(out)))
+        return out
+
+    def double_config(self, cfg):
+        """create_simulation_data.py create_doub_input for one configuration:
+        Ntau doubled, fields resampled, Converged false."""
+        c = dict(cfg)
+        ic = dict(c["Initial_Conditions"])
+        n = int(c["Ntau"])
+        f = self.resample(np.array([ic["fc"], ic["psic"], ic["Up"]]), 2 * n)
+        ic["fc"], ic["psic"], ic["Up"] = f[0].tolist(), f[1].tolist(), f[2].tolist()
+        c["Initial_Conditions"] = ic
+        c["Ntau"] = 2 * n
+        c["Converged"] = False
+        return c
+
     # -- serving ---------------------------------------------------------------
     def serve_start(self, hbm_budget_bytes=0, max_active=0):
         opts = ServeOpts(int(hbm_budget_bytes), int(max_active))
@@ -442,6 +464,20 @@ class Solve:
         self.engine._check(self.lib.pcc_newton_step(self.h, _p(x), ctypes.byref(err), precision, ctypes.byref(st),
                                                     ctypes.byref(rep)))
         return x, err.value, st.as_dict(), rep.as_dict()
+
+    def shoot_debug(self, in0, debug_nx):
+        """shoot + the Debug field export -> (out0, grid indices, fields[k][4][Ntau] = A, U, V, f)."""
+        x = _f64(in0)
+        out = np.zeros(self.nn)
+        cnt = ctypes.c_int(0)
+        # the first call only counts the snapshots
+        self.lib.pcc_shoot_debug(self.h, _p(x), _p(out), int(debug_nx), 0, ctypes.byref(cnt), None, None, None)
+        k = cnt.value
+        idx = np.zeros(k, dtype=np.int32)
+        fields = np.zeros((k, 4, self.ntau))
+        self.engine._check(self.lib.pcc_shoot_debug(self.h, _p(x), _p(out), int(debug_nx), k, ctypes.byref(cnt),
+                                                    idx.ctypes.data_as(_I), _p(fields), None))
+        return out, idx, fields
 
     def newton_begin(self, in0):
         self.engine._check(self.lib.pcc_newton_begin(self.h, _p(_f64(in0))))

@@ -119,3 +119,36 @@ def test_newton_update_reference_consistent(oracle):
     dx, st = oracle.dgesv(d["jac_cols"], -d["out0"])
     assert st == 0
     assert rel_err(dx, d["newton_dx"]) < 1e-9
+
+
+def test_resample_oracle_matches_reference_script():
+    """oracle_py.double_field against the reference's create_simulation_data.py
+    double() (golden vectors made by importing the script)."""
+    import oracle_py
+
+    d = np.load(GOLDEN / "ref_resample_128.npz")
+    for f in ["fc", "psic", "Up"]:
+        x = d[f + "_128"]
+        for n in [256, 512, 1024]:
+            x = oracle_py.double_field(x)
+            assert np.array_equal(x, d[f"{f}_{n}"]), (f, n)
+
+
+def test_suite_goldens_and_quadratic_seeding():
+    """The reference's continuation run (tests/golden/make_suite_golden.py):
+    every dimension converged, and the quadratic seed of D_i (i >= 3) from the
+    previous three converged ones (oracle_py restatement of main.cpp:300-354)
+    lies close to the converged D_i the reference then found."""
+    import oracle_py
+
+    g = np.load(GOLDEN / "ref_suite_128.npz")
+    for b in ["up", "down"]:
+        assert g[f"{b}_converged"].all()
+        dims = [float(k) for k in g[f"{b}_keys"]]
+        assert (np.diff(dims) != 0).all()
+        for i in range(3, len(dims)):
+            prev = [dims[i - 1], dims[i - 2], dims[i - 3]]
+            for f, tol in [("fc", 1e-5), ("Up", 1e-4), ("psic", 1e-3), ("delta", 1e-6)]:
+                v = g[f"{b}_{f}"]
+                seed = oracle_py.quadratic_extrapolate(prev, np.array([v[i - 1], v[i - 2], v[i - 3]]), dims[i])
+                assert np.max(np.abs(seed - v[i])) / np.max(np.abs(v[i])) < tol, (b, i, f)
