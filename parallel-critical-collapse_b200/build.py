@@ -58,7 +58,8 @@ def _compile(unit, force, verbose):
     dep = max(_newest_dep(), src.stat().st_mtime)
     if not force and obj.exists() and obj.stat().st_mtime >= dep:
         return obj, None
-    cmd = [_nvcc()] + NVFLAGS + extra + ["-c", str(src), "-o", str(obj)]
+    user = os.environ.get("PCC_NVCC_EXTRA", "").split()  # extra nvcc flags, e.g. -D options
+    cmd = [_nvcc()] + NVFLAGS + user + extra + ["-c", str(src), "-o", str(obj)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -519,7 +519,8 @@ struct Slot {
     double2* b1;
     int slot_id, lt, s, t;
     bool active;
-    SweepSync sy;
+    SweepSync sy;   // the whole sweep: IRK update, reductions, state hand-over
+    SweepSync gsy;  // this stage group only: the transforms of its RHS evaluation
 
     __device__ __forceinline__ Slot(double2* smem, int tid)
     {
@@ -542,6 +543,23 @@ struct Slot {
             sy.bar_id = 1 + slot_id;
             sy.nthreads = STP;
             sy.mask = 0xffffffffu;
+        }
+        // A stage's transforms exchange data only inside its own group, so
+        // they synchronise the group alone and the groups of a sweep drift
+        // apart between the IRK updates.  Groups of 64 or more threads are
+        // whole warps (ST is then a multiple of 32: no inactive lanes).
+        if constexpr (TG < 32) {
+            gsy.bar_id = 0;
+            gsy.nthreads = TG;
+            gsy.mask = ((1u << TG) - 1u) << ((tid & 31) / TG * TG);
+        } else if constexpr (TG == 32) {
+            gsy.bar_id = 0;
+            gsy.nthreads = 32;
+            gsy.mask = 0xffffffffu;
+        } else {
+            gsy.bar_id = 1 + K::SPC + slot_id * S + s_raw;
+            gsy.nthreads = TG;
+            gsy.mask = 0xffffffffu;
         }
         double2* base = smem + (size_t)slot_id * K::PER_SWEEP;
         ex = base;
@@ -664,7 +682,7 @@ __device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S>& sl, d
         const int max_its = sc.max_its();
         for (int its = 0; its < max_its; ++its) {
             ++its_reached;
-            rhs_eval<N>(ykm, sl.uvm, xs, sc.dim(), sc.dm2c(), k0, t, sl.b0, sl.b1, cur, &sl.lam[s], sc.twN(), sl.sy,
+            rhs_eval<N>(ykm, sl.uvm, xs, sc.dim(), sc.dm2c(), k0, t, sl.b0, sl.b1, cur, &sl.lam[s], sc.twN(), sl.gsy,
                         active, sl.zero);
             sl.sy.sync();  // every stage RHS is in shared memory
             double part = 0.0;
@@ -776,7 +794,7 @@ __global__ void __launch_bounds__(MarchShape<N, S>::NT, MINB) march_kernel(March
             // single RHS evaluation of the state at x_in[item]
             int cur = 0;
             rhs_eval<N>(sl.ykm, sl.uvm, P.x_in[item], P.dim, P.dim_m2_cubed, k0, sl.t, sl.b0, sl.b1, cur,
-                        &sl.lam[sl.s], P.twN, sl.sy, sl.active, sl.zero);
+                        &sl.lam[sl.s], P.twN, sl.gsy, sl.active, sl.zero);
             sl.sy.sync();
             if (sl.active && sl.s == 0) {
                 const double2* fr = cur ? sl.b1 : sl.b0;
