@@ -225,6 +225,39 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+def predictor_build(eng, cfg, in0, out0, J_faithful, steps, flush):
+    """C3 Jacobian builds with the optional stage predictor (each step's
+    fixed-point iteration starts from the previous step's collocation
+    polynomial; not in the reference): builds/s and the difference of its
+    Jacobian from the faithful build, relative to max |J|."""
+    import torch
+
+    import pcc
+
+    s = eng.solve(pcc.SolveDesc.from_config(dict(cfg, IRKPredictor=True)))
+    nn = s.nn
+    d_in0 = torch.tensor(in0, dtype=torch.float64, device="cuda")
+    d_out0 = torch.tensor(out0, dtype=torch.float64, device="cuda")
+    d_J = torch.empty((nn, nn), dtype=torch.float64, device="cuda")
+    s.jacobian_device(d_in0.data_ptr(), d_out0.data_ptr(), d_J.data_ptr())
+    s.sync()
+    ms, rhs = [], 0
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        s.jacobian_device(d_in0.data_ptr(), d_out0.data_ptr(), d_J.data_ptr())
+        st = s.sync()
+        ms.append(st["ms_total"])
+        rhs += st["rhs_evals"]
+    J = d_J.cpu().numpy()
+    s.close()
+    return {"builds_per_s": steps / (float(np.sum(ms)) * 1e-3), "ms_per_build": float(np.mean(ms)),
+            "rhs_evals_per_build": rhs / steps,
+            "J_diff_vs_faithful_rel_max": float(np.max(np.abs(J - J_faithful)) / np.max(np.abs(J_faithful))),
+            "note": "stage iteration started from the previous step's collocation polynomial (not in the "
+                    "reference); same fixed point to PrecisionIRK"}
+
+
 def newton_compare(eng, cfg, in0, out0, J):
     """C3 Newton steps: the batched form (base shoot and all 768 columns in one
     persistent launch, device-side Newton update) with the mixed-precision and
@@ -444,6 +477,8 @@ def run_engine(args, world, rank, local):
                 "flops_per_launch": flops_per_launch, "rhs_evals_per_launch": rhs / args.steps,
                 "flop_convention": "7*5*N*log2(N) + 100*N per RHS evaluation (reference algorithm)"}
 
+    predictor = predictor_build(eng, cfg, in0, out0, h_J.numpy().copy(), args.steps, flush) \
+        if not args.quick else None
     newton = newton_compare(eng, cfg, in0, out0, h_J.numpy().copy()) if not args.quick else None
     dscan = run_dscan(eng, args) if not args.quick else None
     serving = run_serving(eng, args, args.rate, args.requests) if not args.quick else None
@@ -467,7 +502,8 @@ def run_engine(args, world, rank, local):
                            "parallelism": f"{world} independent solves, one per GPU",
                            "sweep_ctas": st_e.sweep_ctas, "wall_s": wall},
                 "clocks": clk, "e2e": e2e, "gpu_launches": 4 * args.steps, "roofline": roofline,
-                "cpu_baseline": cpu, "newton_step": newton, "dscan16": dscan, "serving": serving}
+                "cpu_baseline": cpu, "predictor": predictor, "newton_step": newton, "dscan16": dscan,
+                "serving": serving}
         print(json.dumps(line))
     solve.close()
     eng.close()

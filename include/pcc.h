@@ -69,6 +69,10 @@ typedef struct {
     double prec_newton;  /* PrecisionNewton */
     double slow_error;   /* SlowError (Newton damping) */
     int max_newton;      /* MaxIterNewton */
+    int irk_predictor;   /* start of each step's stage iteration: 0 = y, as the reference
+                          * (ODEStepper.cpp:202-212); 1 = the previous step's collocation
+                          * polynomial, extrapolated (not in the reference: the same fixed
+                          * point to round-off, fewer iterations) */
 } pcc_solve_desc;
 
 typedef struct {

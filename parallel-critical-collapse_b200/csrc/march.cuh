@@ -55,6 +55,8 @@ struct MarchParams {
     int max_its;
     int stages;
     double a[3][3], b[3], c[3];
+    int predictor;                     // 1: stage iteration starts from the extrapolated collocation polynomial
+    double lq[3][3];                   // int_0^theta l_j = sum_k lq[j][k] theta^(k+1) (Lagrange basis on c)
     const double2* __restrict__ twN;   // exp(+2 pi i k/N), k < N
     const double* __restrict__ x_in;   // [item] (modes 1 and 2)
     const double* __restrict__ x_out;  // [item] (mode 2)
@@ -608,6 +610,8 @@ struct ParamScalars {
     __device__ __forceinline__ double a(int i, int j) const { return P.a[i][j]; }
     __device__ __forceinline__ double b(int i) const { return P.b[i]; }
     __device__ __forceinline__ double c(int i) const { return P.c[i]; }
+    __device__ __forceinline__ int predictor() const { return P.predictor; }
+    __device__ __forceinline__ double lq(int j, int k) const { return P.lq[j][k]; }
     __device__ __forceinline__ int mode() const { return P.mode; }
     __device__ __forceinline__ double x_in(int item) const { return P.x_in[item]; }
     __device__ __forceinline__ double x_out(int item) const { return P.x_out[item]; }
@@ -642,6 +646,7 @@ __device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S>& sl, d
     int cur = 0;
     const int nsteps = mode == 2 ? 1 : (side == 0 ? sc.nl() : sc.nr());
     int status = 0, fail_at = -1;
+    double dx_prev = 0.0;
 
     for (int st = 0; st < nsteps; ++st) {
         double xin, xout;
@@ -661,6 +666,41 @@ __device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S>& sl, d
         }
         const double dx = xout - xin;
         const double xs = xin + dx * sc.c(s);
+        if (mode == 0 && st > 0 && sc.predictor()) {
+            // Optional start of the stage iteration (the reference restarts
+            // at y): the previous step's collocation polynomial at this
+            // step's stage abscissae, Y_s = y_{n+1} + h_n sum_j (L_j(theta_s)
+            // - b_j) f_j with theta_s = 1 + c_s h_{n+1} / h_n, L_j the
+            // integrated Lagrange basis on the nodes and f_j the previous
+            // step's last stage derivatives.  ykm holds y_{n+1} here.
+            const double th = 1.0 + sc.c(s) * (dx / dx_prev);
+            double w[S];
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+                double L = 0.0, pw = th;
+#pragma unroll
+                for (int k = 0; k < S; ++k) {
+                    L = fma(sc.lq(j, k), pw, L);
+                    pw *= th;
+                }
+                w[j] = dx_prev * (L - sc.b(j));
+            }
+            if (active) {
+#pragma unroll
+                for (int sg = 0; sg < 8; ++sg) {
+                    double2 y = ykm[sg * TG + t];
+#pragma unroll
+                    for (int j = 0; j < S; ++j) {
+                        const double2 f = ex[(size_t)(j * 2 + cur) * K::MP + sg * TG + t];
+                        y.x = fma(w[j], f.x, y.x);
+                        y.y = fma(w[j], f.y, y.y);
+                    }
+                    ykm[sg * TG + t] = y;
+                }
+            }
+            sl.sy.sync();  // every group has read the stage derivatives
+        }
+        dx_prev = dx;
         if (mode == 0) {
             // the state at the start of this step, for the Debug field export
             // (ShootingSolver.cpp:85-97, 128-138)
@@ -838,6 +878,7 @@ struct BatchSolve {
     const int* cancel;    // optional: nonzero skips the solve's remaining sweeps
     double dim, dm2c, prec;
     int nl, nr, max_its, ntau;
+    int predictor;
 };
 
 constexpr int kBatchMaxClasses = 4;
@@ -850,6 +891,7 @@ struct BatchParams {
     int cls_begin[kBatchMaxClasses + 1];
     int* cls_counter;   // [kBatchMaxClasses]
     double a[3][3], b[3], c[3];
+    double lq[3][3];               // as MarchParams::lq
     unsigned long long* counters;  // [0] RHS evaluations [1] IRK iterations [2] steps
 };
 
@@ -864,6 +906,7 @@ struct SweepScalars {
     int* fail_index;
     double dim, dm2c, prec;
     int nl, nr, max_its, side;
+    int predictor;
 };
 
 struct SmemScalars {
@@ -880,6 +923,8 @@ struct SmemScalars {
     __device__ __forceinline__ double a(int i, int j) const { return B.a[i][j]; }
     __device__ __forceinline__ double b(int i) const { return B.b[i]; }
     __device__ __forceinline__ double c(int i) const { return B.c[i]; }
+    __device__ __forceinline__ int predictor() const { return p->predictor; }
+    __device__ __forceinline__ double lq(int j, int k) const { return B.lq[j][k]; }
     __device__ __forceinline__ int mode() const { return 0; }
     __device__ __forceinline__ double x_in(int) const { return 0.0; }
     __device__ __forceinline__ double x_out(int) const { return 0.0; }
@@ -937,6 +982,7 @@ __device__ __forceinline__ void batch_class(const BatchParams& B, int c, double2
                 sp->nr = so.nr;
                 sp->max_its = so.max_its;
                 sp->side = it.y & 1;
+                sp->predictor = so.predictor;
                 break;
             }
             *sl.item_slot = i;

@@ -79,6 +79,31 @@ int tableau(int scheme, double a[3][3], double b[3], double c[3])
     return 2;
 }
 
+// Integrated Lagrange basis on the Gauss nodes c: int_0^theta l_j(tau) dtau
+// = sum_k lq[j][k] theta^(k+1), l_j(tau) = prod_{m != j} (tau - c_m)/(c_j - c_m).
+// Used by the optional stage predictor of the march.
+void lagrange_integrals(int stages, const double c[3], double lq[3][3])
+{
+    for (int j = 0; j < 3; ++j)
+        for (int k = 0; k < 3; ++k) lq[j][k] = 0.0;
+    for (int j = 0; j < stages; ++j) {
+        double p[3] = {1.0, 0.0, 0.0};  // coefficients of l_j, ascending powers
+        int deg = 0;
+        for (int m = 0; m < stages; ++m) {
+            if (m == j) continue;
+            const double d = c[j] - c[m];
+            double q[3] = {0.0, 0.0, 0.0};
+            for (int k = 0; k <= deg; ++k) {
+                q[k + 1] += p[k] / d;
+                q[k] -= p[k] * c[m] / d;
+            }
+            ++deg;
+            for (int k = 0; k < 3; ++k) p[k] = q[k];
+        }
+        for (int k = 0; k <= deg; ++k) lq[j][k] = p[k] / (k + 1);
+    }
+}
+
 // exp(+2 pi i k/n), k < n, rounded from long-double trigonometry
 std::vector<double2> twiddles(int n)
 {
@@ -149,6 +174,8 @@ MarchParams march_params(pcc_solve* s)
         P.c[i] = s->c[i];
         for (int j = 0; j < 3; ++j) P.a[i][j] = s->a[i][j];
     }
+    P.predictor = s->d.irk_predictor ? 1 : 0;
+    lagrange_integrals(s->stages, s->c, P.lq);
     P.twN = s->d_tw;
     P.status = s->d_status;
     P.fail_index = s->d_fail;
@@ -596,6 +623,7 @@ pcc_status batch_march_items(pcc_ctx* ctx, BatchTables& tab, const std::vector<B
         b.nr = s->d.nr;
         b.max_its = s->d.max_irk;
         b.ntau = s->d.ntau;
+        b.predictor = s->d.irk_predictor ? 1 : 0;
     }
     std::memcpy(h + o_items, table.data(), table.size() * sizeof(int2));
     std::memset(h + o_cls, 0, bytes - o_cls);
@@ -611,6 +639,7 @@ pcc_status batch_march_items(pcc_ctx* ctx, BatchTables& tab, const std::vector<B
         B.c[i] = s0->c[i];
         for (int j = 0; j < 3; ++j) B.a[i][j] = s0->a[i][j];
     }
+    lagrange_integrals(s0->stages, s0->c, B.lq);
     PCC_CUDA(ctx, cudaEventRecord(tab.ev[0], st));
     PCC_CUDA(ctx, launch_march_batch(B, max_ctas, st, &tab.info));
     PCC_CUDA(ctx, cudaEventRecord(tab.ev[1], st));

@@ -19,6 +19,7 @@ struct SimulationConfig {
     Scheme SchemeIRK;
     int MaxIterIRK;
     real_t Delta = 0.0;
+    bool IRKPredictor = false;  // extension key "IRKPredictor" (see pcc_solve_desc::irk_predictor)
     vec_real fc, psic, Up;
 
     explicit SimulationConfig(json in)
@@ -32,6 +33,7 @@ struct SimulationConfig {
         PrecisionNewton = in["PrecisionNewton"];
         SlowError = in["SlowError"];
         MaxIterNewton = in["MaxIterNewton"];
+        if (in.contains("IRKPredictor") && !in["IRKPredictor"].is_null()) IRKPredictor = in["IRKPredictor"];
         Verbose = in["Verbose"];
         Debug = in["Debug"];
         Converged = in["Converged"];
@@ -87,6 +89,7 @@ struct SimulationConfig {
         d.prec_newton = PrecisionNewton;
         d.slow_error = SlowError;
         d.max_newton = MaxIterNewton;
+        d.irk_predictor = IRKPredictor ? 1 : 0;
         return d;
     }
 

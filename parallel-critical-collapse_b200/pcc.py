@@ -54,7 +54,7 @@ class SolveDesc(ctypes.Structure):
                 ("xm", ctypes.c_double), ("xr", ctypes.c_double), ("eps_newton", ctypes.c_double),
                 ("nl", ctypes.c_int), ("nr", ctypes.c_int), ("prec_irk", ctypes.c_double),
                 ("scheme", ctypes.c_int), ("max_irk", ctypes.c_int), ("prec_newton", ctypes.c_double),
-                ("slow_error", ctypes.c_double), ("max_newton", ctypes.c_int)]
+                ("slow_error", ctypes.c_double), ("max_newton", ctypes.c_int), ("irk_predictor", ctypes.c_int)]
 
     @classmethod
     def from_config(cls, cfg):
@@ -63,7 +63,7 @@ class SolveDesc(ctypes.Structure):
                    float(cfg["XRight"]), float(cfg["EpsNewton"]), int(cfg["NLeft"]), int(cfg["NRight"]),
                    float(cfg["PrecisionIRK"]), int(cfg["SchemeIRK"]), int(cfg["MaxIterIRK"]),
                    float(cfg.get("PrecisionNewton", 1e-14)), float(cfg.get("SlowError", 1e-3)),
-                   int(cfg.get("MaxIterNewton", 100)))
+                   int(cfg.get("MaxIterNewton", 100)), int(bool(cfg.get("IRKPredictor", False))))
 
 
 class Stats(ctypes.Structure):
