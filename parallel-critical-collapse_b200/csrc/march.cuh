@@ -81,11 +81,15 @@ struct MarchShape {
     static constexpr int NT = SPC * STP;                      // threads per CTA
     static constexpr int NW = STP >= 32 ? STP / 32 : 1;       // warps per sweep
     static constexpr int MP = M;                              // exchange length (swizzled)
-    static constexpr int EX = S * 2 * MP;                     // exchange double2s
+    static constexpr int EXA = S * 2 * MP;                    // exchange pairs of the first transform
     static constexpr int YS = 8 * TG;                         // slot-indexed y
     static constexpr int YK = S * 8 * TG;                     // slot-indexed stage values
     static constexpr int UV = S * M;                          // U and V per stage (doubles -> M double2)
     static constexpr int MISC = (S + NW + 1) / 2 + 2;          // lam, red, item, zero (in double2)
+    // paired transforms (dft_m2) need a second set of exchange pairs; shapes
+    // whose shared memory would not fit keep single transforms
+    static constexpr bool DUAL = (size_t)SPC * (2 * EXA + YS + YK + UV + MISC) * 16 <= 200 * 1024;
+    static constexpr int EX = DUAL ? 2 * EXA : EXA;           // exchange double2s
     static constexpr int PER_SWEEP = EX + YS + YK + UV + MISC; // double2 per sweep
     static constexpr size_t SMEM = (size_t)SPC * PER_SWEEP * sizeof(double2);
     static constexpr int NP = M == 64 ? 2 : (M <= 512 ? 3 : 4);
@@ -275,6 +279,88 @@ __device__ __forceinline__ void dft_m(double2 (&v)[8], double2* __restrict__ b0,
     }
 }
 
+// Two independent length-M DFTs of the same direction in one set of passes:
+// the same arithmetic as two dft_m calls, with one twiddle fetch and one
+// barrier per pass for both and twice the independent work between barriers.
+// v uses the buffer pair (a0, a1), u the pair (c0, c1), both selected by cur.
+template <int M, int TG, int SG>
+__device__ __forceinline__ void dft_m2(double2 (&v)[8], double2 (&u)[8], double2* __restrict__ a0,
+                                       double2* __restrict__ a1, double2* __restrict__ c0,
+                                       double2* __restrict__ c1, int& cur, int t, const double2* __restrict__ twN,
+                                       const SweepSync& sy, bool active, const volatile int* zero,
+                                       double2* pj = nullptr)
+{
+    constexpr int NP = M == 64 ? 2 : (M <= 512 ? 3 : 4);
+    constexpr int RL = M == 64 ? 8 : M == 128 ? 2 : M == 256 ? 4 : M == 512 ? 8 : 2;
+    const int zoff = *zero;
+    double2* wa0 = cur ? a1 : a0;
+    double2* wa1 = cur ? a0 : a1;
+    double2* wc0 = cur ? c1 : c0;
+    double2* wc1 = cur ? c0 : c1;
+    double2 tw[7];
+    if (active) {
+        stockham_pass<M, TG, 8, 1, SG, false>(v, wa0, t, tw);
+        stockham_pass<M, TG, 8, 1, SG, false>(u, wc0, t, tw);
+    }
+    if constexpr (NP == 2) {
+        if (active) fetch_twiddles<M, TG, RL, 8, SG>(tw, t, twN, zoff);
+        if (pj && active) fetch_point_twiddles<TG>(pj, t, twN, zoff);
+        sy.sync();
+        if (active) {
+            load_std<TG>(v, wa0, t);
+            load_std<TG>(u, wc0, t);
+            stockham_pass<M, TG, RL, 8, SG, true>(v, wa0, t, tw);
+            stockham_pass<M, TG, RL, 8, SG, true>(u, wc0, t, tw);
+        }
+        cur ^= 1;
+    } else if constexpr (NP == 3) {
+        if (active) fetch_twiddles<M, TG, 8, 8, SG>(tw, t, twN, zoff);
+        sy.sync();
+        if (active) {
+            load_std<TG>(v, wa0, t);
+            load_std<TG>(u, wc0, t);
+            stockham_pass<M, TG, 8, 8, SG, false>(v, wa1, t, tw);
+            stockham_pass<M, TG, 8, 8, SG, false>(u, wc1, t, tw);
+            fetch_twiddles<M, TG, RL, 64, SG>(tw, t, twN, zoff);
+        }
+        if (pj && active) fetch_point_twiddles<TG>(pj, t, twN, zoff);
+        sy.sync();
+        if (active) {
+            load_std<TG>(v, wa1, t);
+            load_std<TG>(u, wc1, t);
+            stockham_pass<M, TG, RL, 64, SG, true>(v, wa1, t, tw);
+            stockham_pass<M, TG, RL, 64, SG, true>(u, wc1, t, tw);
+        }
+    } else {
+        if (active) fetch_twiddles<M, TG, 8, 8, SG>(tw, t, twN, zoff);
+        sy.sync();
+        if (active) {
+            load_std<TG>(v, wa0, t);
+            load_std<TG>(u, wc0, t);
+            stockham_pass<M, TG, 8, 8, SG, false>(v, wa1, t, tw);
+            stockham_pass<M, TG, 8, 8, SG, false>(u, wc1, t, tw);
+            fetch_twiddles<M, TG, 8, 64, SG>(tw, t, twN, zoff);
+        }
+        sy.sync();
+        if (active) {
+            load_std<TG>(v, wa1, t);
+            load_std<TG>(u, wc1, t);
+            stockham_pass<M, TG, 8, 64, SG, false>(v, wa0, t, tw);
+            stockham_pass<M, TG, 8, 64, SG, false>(u, wc0, t, tw);
+            fetch_twiddles<M, TG, RL, 512, SG>(tw, t, twN, zoff);
+        }
+        if (pj && active) fetch_point_twiddles<TG>(pj, t, twN, zoff);
+        sy.sync();
+        if (active) {
+            load_std<TG>(v, wa0, t);
+            load_std<TG>(u, wc0, t);
+            stockham_pass<M, TG, RL, 512, SG, true>(v, wa0, t, tw);
+            stockham_pass<M, TG, RL, 512, SG, true>(u, wc0, t, tw);
+        }
+        cur ^= 1;
+    }
+}
+
 // --------------------------------------------------------------- slot maps
 // Slot sigma = 2*ri + parity; ri -> position q in {0, 1, 6, 7}; parity 0 odd
 // modes, 1 even modes.  Returns the state mode index (0..M-1).
@@ -305,10 +391,14 @@ __device__ __forceinline__ int slot_q(int sigma)
 // ODEStepper.cpp:92-136).  yks: this stage's slot-indexed state (shared);
 // b0/b1: this stage's exchange buffers; the result is written slot-indexed
 // into (cur ? b1 : b0), the buffer the next transform would write first.
-template <int N>
+// DUAL: the three pairs of independent transforms (U+iV with F, the last IA2
+// transform with dU+idV, the odd with the even forward transform) run as
+// paired transforms (dft_m2) through the second exchange pair c0/c1.
+template <int N, bool DUAL>
 __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double* __restrict__ uvs, double x,
                                          double dim, double dm2c, double k0, int t, double2* __restrict__ b0,
-                                         double2* __restrict__ b1, int& cur, double* lam_slot,
+                                         double2* __restrict__ b1, double2* __restrict__ c0,
+                                         double2* __restrict__ c1, int& cur, double* lam_slot,
                                          const double2* __restrict__ twN, const SweepSync& sy, bool active,
                                          const volatile int* zero)
 {
@@ -318,6 +408,22 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
     double F[8];
     double* Us = uvs;      // [q][t], this thread's own entries only
     double* Vs = uvs + M;
+
+    double2 u[8];  // the second transform of a pair (DUAL)
+    // F from the even modes: doubleModes (with its N/4 quirk) + phase fix
+    auto even_input = [&](double2 (&w)[8]) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) w[q] = make_double2(0.0, 0.0);
+        if (active) {
+            w[0] = yks[1 * TG + t];
+            if (t == 1) w[0].x = -yks[7 * TG + TG - 1].x;  // Re c[2] = -Re c[N-2] = -Re Y[M-2]
+            w[1] = yks[3 * TG + t];
+            const double2 yq = yks[5 * TG + t];
+            if (t == 0) w[2] = make_double2(0.5 * yq.x, 0.5 * yq.y);  // c[N/4] = Y[N/4]/2
+            w[6] = yq;                                                  // c[3N/4] = Y[N/4] (t = 0)
+            w[7] = yks[7 * TG + t];
+        }
+    };
 
     // --- U + iV from the odd modes (IDFT_M, post-twiddle w^j) ----------------
 #pragma unroll
@@ -329,7 +435,12 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
         v[7] = yks[6 * TG + t];
     }
     double2 pj[8];
-    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero, pj);
+    if constexpr (DUAL) {
+        even_input(u);
+        dft_m2<M, TG, -1>(v, u, b0, b1, c0, c1, cur, t, twN, sy, active, zero, pj);
+    } else {
+        dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero, pj);
+    }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         const double2 o = cmul(v[q], cconj(pj[q]));
@@ -339,21 +450,16 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
         }
     }
 
-    // --- F from the even modes: doubleModes (with its N/4 quirk) + phase fix --
+    // --- F ---------------------------------------------------------------------
+    if constexpr (DUAL) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = make_double2(0.0, 0.0);
-    if (active) {
-        v[0] = yks[1 * TG + t];
-        if (t == 1) v[0].x = -yks[7 * TG + TG - 1].x;  // Re c[2] = -Re c[N-2] = -Re Y[M-2]
-        v[1] = yks[3 * TG + t];
-        const double2 yq = yks[5 * TG + t];
-        if (t == 0) v[2] = make_double2(0.5 * yq.x, 0.5 * yq.y);  // c[N/4] = Y[N/4]/2
-        v[6] = yq;                                                  // c[3N/4] = Y[N/4] (t = 0)
-        v[7] = yks[7 * TG + t];
+        for (int q = 0; q < 8; ++q) F[q] = u[q].y;
+    } else {
+        even_input(v);
+        dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) F[q] = v[q].y;
     }
-    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) F[q] = v[q].y;
 
     // --- IA2 constraint coefficients (InitialConditionGenerator.cpp:876-881) --
     const double c8 = dm2c / (8.0 * x);  // (D-2)^3 / (8x), once per evaluation
@@ -415,26 +521,37 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
             }
         }
     }
-    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
-    double IA2[8];
+    // dU + i dV from -i m k0 c on the odd modes
+    auto du_input = [&](double2 (&w)[8]) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) IA2[q] = v[q].x * Fr[q];  // X e^{-F}
-
-    // --- dU + i dV from -i m k0 c on the odd modes ---------------------------
+        for (int q = 0; q < 8; ++q) w[q] = make_double2(0.0, 0.0);
+        if (active) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = make_double2(0.0, 0.0);
-    if (active) {
-#pragma unroll
-        for (int ri = 0; ri < 4; ++ri) {
-            const int q = ri < 2 ? ri : ri + 4;
-            const int k = 2 * (t + TG * q) + 1;
-            const int m = k < M ? k : k - N;
-            const double s = m * k0;
-            const double2 a = yks[(2 * ri) * TG + t];
-            v[q] = make_double2(s * a.y, -(s * a.x));
+            for (int ri = 0; ri < 4; ++ri) {
+                const int q = ri < 2 ? ri : ri + 4;
+                const int k = 2 * (t + TG * q) + 1;
+                const int m = k < M ? k : k - N;
+                const double s = m * k0;
+                const double2 a = yks[(2 * ri) * TG + t];
+                w[q] = make_double2(s * a.y, -(s * a.x));
+            }
         }
+    };
+    double IA2[8];
+    if constexpr (DUAL) {
+        du_input(u);
+        dft_m2<M, TG, -1>(v, u, b0, b1, c0, c1, cur, t, twN, sy, active, zero, pj);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) IA2[q] = v[q].x * Fr[q];  // X e^{-F}
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = u[q];
+    } else {
+        dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) IA2[q] = v[q].x * Fr[q];  // X e^{-F}
+        du_input(v);
+        dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero, pj);
     }
-    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero, pj);
 
     // --- pointwise Einstein-scalar RHS (ODEStepper.cpp:109-122) ---------------
     // divisions are taken as reciprocals shared between terms (one for 1/IA2,
@@ -457,30 +574,41 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
         v[q] = cmul(make_double2(ux, vx), w);  // pre-twiddle exp(+2 pi i j/N)
     }
 
-    // --- FieldsToStateVector: odd modes ---------------------------------------
-    dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
-    const double2 o0 = make_double2(v[0].x * invM, v[0].y * invM);
-    const double2 o1 = make_double2(v[1].x * invM, v[1].y * invM);
-    const double2 o6 = make_double2(v[6].x * invM, v[6].y * invM);
-    const double2 o7 = make_double2(v[7].x * invM, v[7].y * invM);
-    // --- even modes, halveModes fold of N/4 and 3N/4, frozen Delta slot ---------
+    // --- FieldsToStateVector: odd modes, then the even modes with the
+    // halveModes fold of N/4 and 3N/4 and the frozen Delta slot ----------------
+    auto write_f = [&](const double2 (&od)[8], const double2 (&ev)[8]) {
+        if (active) {
+            double2* fslot = cur ? b1 : b0;
+            double2 e0 = make_double2(ev[0].x * invM, ev[0].y * invM);
+            if (t == 1) e0.x = 0.0;  // dYdx[2] real part (Delta) frozen
+            double2 e6 = make_double2(ev[6].x * invM, ev[6].y * invM);
+            if (t == 0) e6 = cadd(make_double2(ev[2].x * invM, ev[2].y * invM), e6);  // in[N/4] + in[3N/4]
+            fslot[0 * TG + t] = od[0];
+            fslot[1 * TG + t] = e0;
+            fslot[2 * TG + t] = od[1];
+            fslot[3 * TG + t] = make_double2(ev[1].x * invM, ev[1].y * invM);
+            fslot[4 * TG + t] = od[6];
+            fslot[5 * TG + t] = e6;
+            fslot[6 * TG + t] = od[7];
+            fslot[7 * TG + t] = make_double2(ev[7].x * invM, ev[7].y * invM);
+        }
+    };
+    if constexpr (DUAL) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = make_double2(0.0, fx[q]);
-    dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
-    if (active) {
-        double2* fslot = cur ? b1 : b0;
-        double2 e0 = make_double2(v[0].x * invM, v[0].y * invM);
-        if (t == 1) e0.x = 0.0;  // dYdx[2] real part (Delta) frozen
-        double2 e6 = make_double2(v[6].x * invM, v[6].y * invM);
-        if (t == 0) e6 = cadd(make_double2(v[2].x * invM, v[2].y * invM), e6);  // in[N/4] + in[3N/4]
-        fslot[0 * TG + t] = o0;
-        fslot[1 * TG + t] = e0;
-        fslot[2 * TG + t] = o1;
-        fslot[3 * TG + t] = make_double2(v[1].x * invM, v[1].y * invM);
-        fslot[4 * TG + t] = o6;
-        fslot[5 * TG + t] = e6;
-        fslot[6 * TG + t] = o7;
-        fslot[7 * TG + t] = make_double2(v[7].x * invM, v[7].y * invM);
+        for (int q = 0; q < 8; ++q) u[q] = make_double2(0.0, fx[q]);
+        dft_m2<M, TG, 1>(v, u, b0, b1, c0, c1, cur, t, twN, sy, active, zero);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = make_double2(v[q].x * invM, v[q].y * invM);
+        write_f(v, u);
+    } else {
+        dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
+        double2 od[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) od[q] = make_double2(v[q].x * invM, v[q].y * invM);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = make_double2(0.0, fx[q]);
+        dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
+        write_f(od, v);
     }
 }
 
@@ -519,6 +647,8 @@ struct Slot {
     volatile int* zero;
     double2* b0;
     double2* b1;
+    double2* c0;  // the second transform's exchange pair (K::DUAL)
+    double2* c1;
     int slot_id, lt, s, t;
     bool active;
     SweepSync sy;   // the whole sweep: IRK update, reductions, state hand-over
@@ -575,6 +705,8 @@ struct Slot {
         zero = item_slot + 1;
         b0 = ex + (size_t)s * 2 * K::MP;
         b1 = b0 + K::MP;
+        c0 = ex + K::EXA + (size_t)s * 2 * K::MP;
+        c1 = c0 + K::MP;
         ykm = yks + (size_t)s * 8 * TG;
         uvm = uv + (size_t)s * 2 * K::M;
     }
@@ -722,8 +854,8 @@ __device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S>& sl, d
         const int max_its = sc.max_its();
         for (int its = 0; its < max_its; ++its) {
             ++its_reached;
-            rhs_eval<N>(ykm, sl.uvm, xs, sc.dim(), sc.dm2c(), k0, t, sl.b0, sl.b1, cur, &sl.lam[s], sc.twN(), sl.gsy,
-                        active, sl.zero);
+            rhs_eval<N, K::DUAL>(ykm, sl.uvm, xs, sc.dim(), sc.dm2c(), k0, t, sl.b0, sl.b1, sl.c0, sl.c1, cur,
+                                 &sl.lam[s], sc.twN(), sl.gsy, active, sl.zero);
             sl.sy.sync();  // every stage RHS is in shared memory
             double part = 0.0;
             if (active) {
@@ -833,8 +965,8 @@ __global__ void __launch_bounds__(MarchShape<N, S>::NT, MINB) march_kernel(March
         if (P.mode == 1) {
             // single RHS evaluation of the state at x_in[item]
             int cur = 0;
-            rhs_eval<N>(sl.ykm, sl.uvm, P.x_in[item], P.dim, P.dim_m2_cubed, k0, sl.t, sl.b0, sl.b1, cur,
-                        &sl.lam[sl.s], P.twN, sl.gsy, sl.active, sl.zero);
+            rhs_eval<N, K::DUAL>(sl.ykm, sl.uvm, P.x_in[item], P.dim, P.dim_m2_cubed, k0, sl.t, sl.b0, sl.b1,
+                                 sl.c0, sl.c1, cur, &sl.lam[sl.s], P.twN, sl.gsy, sl.active, sl.zero);
             sl.sy.sync();
             if (sl.active && sl.s == 0) {
                 const double2* fr = cur ? sl.b1 : sl.b0;
