@@ -170,15 +170,105 @@ def barrier(world):
         dist.barrier()
 
 
+def _dist_device():
+    import torch.distributed as dist
+
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
 def max_over_ranks(world, v):
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device=_dist_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def column_blocks(nn, world):
+    """Contiguous column partition of a Jacobian over `world` ranks (block
+    sizes differ by at most one)."""
+    base, extra = divmod(nn, world)
+    out, c = [], 0
+    for r in range(world):
+        k = base + (1 if r < extra else 0)
+        out.append((c, c + k))
+        c += k
+    return out
+
+
+def gather_columns(local, nn, blocks, world):
+    """All-gather of the ranks' column-major blocks (each padded to the largest
+    block) -> the full J, row-major, on every rank."""
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+
+        parts = [torch.empty_like(local) for _ in range(world)]
+        dist.all_gather(parts, local)
+    else:
+        parts = [local]
+    cols = [parts[r][:(c1 - c0) * nn].view(c1 - c0, nn) for r, (c0, c1) in enumerate(blocks)]
+    return torch.cat(cols, 0).t().contiguous()
+
+
+def run_shard(args, world, rank, local):
+    """One Jacobian split over the ranks (SURVEY-style column sharding): every
+    rank builds its contiguous block of columns of the same seeded C3 solve
+    with one persistent launch, then one all-gather assembles J on every GPU.
+    Strong scaling; time = max over ranks of (build + gather) device time."""
+    import torch
+
+    import pcc
+
+    torch.cuda.set_device(local)
+    eng = pcc.Engine(local)
+    cfg, in0 = workload(args.seed, args.amp)  # the same solve on every rank
+    solve = eng.solve(pcc.SolveDesc.from_config(cfg))
+    nn = solve.nn
+    out0 = solve.shoot(in0)
+    blocks = column_blocks(nn, world)
+    c0, c1 = blocks[rank]
+    nb = max(b - a for a, b in blocks)
+    d_in0 = torch.tensor(in0, dtype=torch.float64, device="cuda")
+    d_out0 = torch.tensor(out0, dtype=torch.float64, device="cuda")
+    d_cols = torch.zeros(nb * nn, dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def step():
+        solve.jacobian_columns_device(d_in0.data_ptr(), d_out0.data_ptr(), c0, c1, d_cols.data_ptr())
+        st = solve.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        J = gather_columns(d_cols, nn, blocks, world)
+        e1.record()
+        torch.cuda.synchronize()
+        return st["ms_total"] + e0.elapsed_time(e1), J
+
+    for _ in range(args.warmup):
+        step()
+    barrier(world)
+    ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        barrier(world)
+        t, J = step()
+        ms.append(t)
+    total = max_over_ranks(world, float(np.sum(ms)))
+    finite = bool(torch.isfinite(J).all().item())
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": args.steps / (total * 1e-3), "unit": "builds/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": total / args.steps, "higher_is_better": True, "scaling": "strong",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded free data)",
+                          "config": {"workload": "C3 Jacobian, columns sharded over the GPUs, one all-gather",
+                                     "blocks": blocks, "finite": finite}}))
+    solve.close()
+    eng.close()
 
 
 def cpu_reference(cfg, in0, out0, columns, threads):
@@ -522,6 +612,9 @@ def main():
     ap.add_argument("--rate", type=float, default=4.0, help="C5 Poisson arrival rate (requests/s)")
     ap.add_argument("--requests", type=int, default=16, help="C5 requests")
     ap.add_argument("--dscan-amp", type=float, default=0.01, help="C4 free-data perturbation amplitude")
+    ap.add_argument("--shard", choices=["solves", "columns"], default="solves",
+                    help="multi-GPU: independent solves per GPU (weak scaling, default) or one Jacobian's "
+                         "columns split over the GPUs and all-gathered (strong scaling)")
     ap.add_argument("--columns", type=int, default=0,
                     help="profiling aid: build only the first C columns (not a benchmark line)")
     args = ap.parse_args()
@@ -529,6 +622,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.shard == "columns":
+            run_shard(args, world, rank, local)
         else:
             run_engine(args, world, rank, local)
     finally:

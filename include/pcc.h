@@ -134,6 +134,14 @@ pcc_status pcc_jacobian(pcc_solve* s, const double* in0, const double* out0, dou
 pcc_status pcc_jacobian_device(pcc_solve* s, const double* d_in0, const double* d_out0, double* d_J);
 pcc_status pcc_solve_sync(pcc_solve* s, pcc_stats* stats);
 
+/* Columns [c0, c1) of J on device pointers, written column-major
+ * (d_cols[(c - c0) * Nnewton + row] = J[row][c]), so that the blocks of a
+ * column partition concatenate into J^T: the building block of a Jacobian
+ * sharded over several GPUs and gathered with one all-gather.  Asynchronous
+ * on the context stream; stats after pcc_solve_sync. */
+pcc_status pcc_jacobian_columns_device(pcc_solve* s, const double* d_in0, const double* d_out0, int c0, int c1,
+                                       double* d_cols);
+
 /* Columns [c0, c1) only (c1 may be Nnewton+1 to include the base shoot, whose
  * output then lands in out_base).  cols is column-major (c1-c0) x Nnewton. */
 pcc_status pcc_jacobian_columns(pcc_solve* s, const double* in0, const double* out0, int c0, int c1,

@@ -613,6 +613,25 @@ cudaError_t launch_epilogue(const BoundaryParams& P, int ctas, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// Finite differences of columns in column-major order (no transpose):
+// cols[i nn + row] = (outc[i nn + row] - out0[row]) / eps, i < ncols.
+__global__ void fd_cols_kernel(const double* __restrict__ outc, const double* __restrict__ out0, double* cols,
+                               int nn, int ncols, double eps)
+{
+    const size_t total = (size_t)ncols * nn;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x)
+        cols[i] = (outc[i] - out0[i % nn]) / eps;
+}
+
+cudaError_t launch_fd_cols(const double* outc, const double* out0, double* cols, int nn, int ncols, double eps,
+                           cudaStream_t st)
+{
+    const size_t total = (size_t)ncols * nn;
+    const int blocks = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
+    fd_cols_kernel<<<blocks < 1 ? 1 : blocks, 256, 0, st>>>(outc, out0, cols, nn, ncols, eps);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fd(const double* outc, const double* out0, double* J, int nn, int c0, int ncols, double eps,
                       cudaStream_t st)
 {

@@ -841,6 +841,27 @@ pcc_status pcc_jacobian_device(pcc_solve* s, const double* d_in0, const double* 
     return PCC_OK;
 }
 
+pcc_status pcc_jacobian_columns_device(pcc_solve* s, const double* d_in0, const double* d_out0, int c0, int c1,
+                                       double* d_cols)
+{
+    if (!s || !d_in0 || !d_out0 || !d_cols) return PCC_ERR_INVALID_ARG;
+    if (c0 < 0 || c1 > s->nn || c0 >= c1) return fail(s->ctx, PCC_ERR_INVALID_ARG, "column range");
+    pcc_ctx* ctx = s->ctx;
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int nn = s->nn;
+    if (d_in0 != s->d_in0)
+        PCC_CUDA(ctx, cudaMemcpyAsync(s->d_in0, d_in0, nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    if (d_out0 != s->d_out0)
+        PCC_CUDA(ctx, cudaMemcpyAsync(s->d_out0, d_out0, nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    pcc_status r = enqueue_columns(s, c0, c1, false, nullptr);
+    if (r != PCC_OK) return r;
+    PCC_CUDA(ctx, launch_fd_cols(s->d_outc, s->d_out0, d_cols, nn, c1 - c0, s->d.eps_newton, ctx->stream));
+    s->pend_c0 = c0;
+    s->pend_c1 = c1;
+    s->pending = true;
+    return PCC_OK;
+}
+
 pcc_status pcc_solve_sync(pcc_solve* s, pcc_stats* stats)
 {
     if (!s) return PCC_ERR_INVALID_ARG;

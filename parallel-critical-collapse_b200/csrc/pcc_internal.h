@@ -24,6 +24,8 @@ cudaError_t launch_double_fields(int n, int count, const double* in, double* out
 // Debug field export: count state snapshots at xs -> fields [count][4][ntau] = A, U, V, f.
 cudaError_t launch_debug_fields(int ntau, double dim, double dm2c, int count, const double* states, const double* xs,
                                 double* fields, double* scratch, int ctas, const double2* tw, cudaStream_t st);
+cudaError_t launch_fd_cols(const double* outc, const double* out0, double* cols, int nn, int ncols, double eps,
+                           cudaStream_t st);
 cudaError_t launch_fd(const double* outc, const double* out0, double* J, int nn, int c0, int ncols, double eps,
                       cudaStream_t st);
 

@@ -37,7 +37,7 @@ EXPORTS = ["pcc_ctx_create", "pcc_ctx_destroy", "pcc_status_string", "pcc_last_e
            "pcc_unpack_fields", "pcc_expansions", "pcc_solve_set_grid", "pcc_dft", "pcc_expansions_static",
            "pcc_jacobian_batch", "pcc_newton_begin", "pcc_newton_iterate", "pcc_newton_result",
            "pcc_newton_solve", "pcc_serve_start", "pcc_submit", "pcc_poll", "pcc_wait", "pcc_serve_stats",
-           "pcc_serve_stop", "pcc_resample_fields", "pcc_shoot_debug"]
+           "pcc_serve_stop", "pcc_resample_fields", "pcc_shoot_debug", "pcc_jacobian_columns_device"]
 
 NEWTON_CODES = ["RUNNING", "CONVERGED", "STOPPED", "MAX_ITER", "IRK_FAILED", "DELTA_MISMATCH", "SINGULAR"]
 
@@ -180,6 +180,7 @@ def load(path=None):
     L.pcc_serve_stop.argtypes = [vp]
     L.pcc_resample_fields.argtypes = [vp, ci, ci, ci, _D, _D]
     L.pcc_shoot_debug.argtypes = [vp, _D, _D, ci, ci, _I, _I, _D, ctypes.POINTER(Stats)]
+    L.pcc_jacobian_columns_device.argtypes = [vp, vp, vp, ci, ci, vp]
     for name in EXPORTS:
         if name not in ("pcc_status_string", "pcc_last_error"):
             getattr(L, name).restype = ci
@@ -450,6 +451,12 @@ class Solve:
         """Asynchronous build on device pointers (ints); pair with sync()."""
         self.engine._check(self.lib.pcc_jacobian_device(self.h, ctypes.c_void_p(d_in0), ctypes.c_void_p(d_out0),
                                                         ctypes.c_void_p(d_J)))
+
+    def jacobian_columns_device(self, d_in0, d_out0, c0, c1, d_cols):
+        """Columns [c0, c1) into device memory d_cols, column-major; finish with sync()."""
+        self.engine._check(self.lib.pcc_jacobian_columns_device(self.h, ctypes.c_void_p(d_in0),
+                                                                ctypes.c_void_p(d_out0), c0, c1,
+                                                                ctypes.c_void_p(d_cols)))
 
     def sync(self):
         st = Stats()

@@ -127,3 +127,23 @@ def test_device_newton_reports_irk_failure(engine):
     assert st[1]["state"] == "IRK_FAILED" and st[1]["fail_column"] >= 0 and st[1]["fail_grid_index"] >= 0
     assert np.array_equal(xs[1], d["in0"])  # no update applied
     assert st[0]["state"] == "MAX_ITER"
+
+
+def test_jacobian_columns_device_blocks(engine):
+    """pcc_jacobian_columns_device: column blocks of J on the device, column-
+    major, as a column-sharded build over several GPUs uses them; the same
+    bits as the corresponding columns of pcc_jacobian."""
+    import torch
+
+    d = load_case("c1_fixture")
+    s = _solve(engine, d["cfg"])
+    nn = s.nn
+    out0 = s.shoot(d["in0"])
+    J = s.jacobian(d["in0"], out0)
+    din = torch.tensor(d["in0"], dtype=torch.float64, device="cuda")
+    dout = torch.tensor(out0, dtype=torch.float64, device="cuda")
+    for c0, c1 in [(0, 40), (40, nn)]:
+        cols = torch.zeros((c1 - c0) * nn, dtype=torch.float64, device="cuda")
+        s.jacobian_columns_device(din.data_ptr(), dout.data_ptr(), c0, c1, cols.data_ptr())
+        s.sync()
+        assert np.array_equal(cols.cpu().numpy().reshape(c1 - c0, nn).T, J[:, c0:c1])
