@@ -278,7 +278,8 @@ cudaError_t lu_solve_fp64(const double* dA, const double* db, double* dx, int n,
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     int zero = 0;
-    return cudaMemcpyAsync(info + 1, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+    (void)zero;
+    return cudaMemsetAsync(info + 1, 0, sizeof(int), st);  // no host source: capturable
 }
 
 cudaError_t lu_solve_mixed(const double* dA, const double* db, double* dx, int n, void* work, size_t work_bytes,

@@ -237,16 +237,27 @@ pcc_status enqueue_epilogue(pcc_solve* s, int c0, int c1, bool fd, double* d_J, 
     return PCC_OK;
 }
 
+// Records ev on st; while st is being captured into a CUDA graph the record
+// becomes an external event node, so that it still timestamps each replay.
+cudaError_t record_event(cudaEvent_t ev, cudaStream_t st)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess) return e;
+    return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal)
+                                               : cudaEventRecord(ev, st);
+}
+
 // Enqueues the build pipeline for columns [c0, c1) reading d_in0 (and d_out0
 // for the differences when fd is set).  Events bracket the stages.
 pcc_status enqueue_columns(pcc_solve* s, int c0, int c1, bool fd, double* d_J)
 {
     pcc_ctx* ctx = s->ctx;
     cudaStream_t st = ctx->stream;
-    PCC_CUDA(ctx, cudaEventRecord(s->ev[0], st));
+    PCC_CUDA(ctx, record_event(s->ev[0], st));
     pcc_status r = enqueue_prologue(s, c0, c1, st);
     if (r != PCC_OK) return r;
-    PCC_CUDA(ctx, cudaEventRecord(s->ev[1], st));
+    PCC_CUDA(ctx, record_event(s->ev[1], st));
     MarchParams P = march_params(s);
     P.n_items = 2 * (c1 - c0);
     P.mode = 0;
@@ -254,10 +265,10 @@ pcc_status enqueue_columns(pcc_solve* s, int c0, int c1, bool fd, double* d_J)
     P.yfinal = s->d_yfinal;
     P.work_counter = s->d_counters_i + 1;
     PCC_CUDA(ctx, launch_march(s->d.ntau, s->stages, P, 0, st, &s->last_launch));
-    PCC_CUDA(ctx, cudaEventRecord(s->ev[2], st));
+    PCC_CUDA(ctx, record_event(s->ev[2], st));
     r = enqueue_epilogue(s, c0, c1, fd, d_J, st);
     if (r != PCC_OK) return r;
-    PCC_CUDA(ctx, cudaEventRecord(s->ev[3], st));
+    PCC_CUDA(ctx, record_event(s->ev[3], st));
     return PCC_OK;
 }
 
@@ -512,6 +523,7 @@ void solve_release(pcc_solve* s)
         }
     for (auto& ev : s->ev)
         if (ev) cudaEventDestroy(ev);
+    if (s->build_graph) cudaGraphExecDestroy(s->build_graph);
     delete s;
 }
 
@@ -829,12 +841,39 @@ pcc_status pcc_jacobian_device(pcc_solve* s, const double* d_in0, const double* 
     pcc_ctx* ctx = s->ctx;
     PCC_CUDA(ctx, cudaSetDevice(ctx->device));
     const int nn = s->nn;
-    if (d_in0 != s->d_in0)
-        PCC_CUDA(ctx, cudaMemcpyAsync(s->d_in0, d_in0, nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-    if (d_out0 != s->d_out0)
-        PCC_CUDA(ctx, cudaMemcpyAsync(s->d_out0, d_out0, nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-    pcc_status r = enqueue_columns(s, 0, nn, true, d_J);
-    if (r != PCC_OK) return r;
+    cudaStream_t st = ctx->stream;
+    auto enqueue = [&]() -> pcc_status {
+        if (d_in0 != s->d_in0)
+            PCC_CUDA(ctx, cudaMemcpyAsync(s->d_in0, d_in0, nn * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        if (d_out0 != s->d_out0)
+            PCC_CUDA(ctx, cudaMemcpyAsync(s->d_out0, d_out0, nn * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        return enqueue_columns(s, 0, nn, true, d_J);
+    };
+    // The build is captured once per set of pointers into a CUDA graph and
+    // replayed: one graph launch for the copies, counter resets, boundary
+    // kernels, the persistent march and the differencing.
+    const void* key[3] = {d_in0, d_out0, d_J};
+    if (!s->build_graph || std::memcmp(key, s->graph_key, sizeof(key)) != 0) {
+        if (s->build_graph) cudaGraphExecDestroy(s->build_graph);
+        s->build_graph = nullptr;
+        cudaGraph_t g = nullptr;
+        PCC_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const pcc_status r = enqueue();
+        const cudaError_t ec = cudaStreamEndCapture(st, &g);
+        if (r != PCC_OK) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (ec != cudaSuccess) return fail(ctx, PCC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+        const cudaError_t ei = cudaGraphInstantiate(&s->build_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            s->build_graph = nullptr;
+            return fail(ctx, PCC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+        }
+        std::memcpy(s->graph_key, key, sizeof(key));
+    }
+    PCC_CUDA(ctx, cudaGraphLaunch(s->build_graph, st));
     s->pend_c0 = 0;
     s->pend_c1 = nn;
     s->pending = true;

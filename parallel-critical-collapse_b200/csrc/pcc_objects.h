@@ -83,6 +83,10 @@ struct pcc_solve {
     int pend_c0 = 0, pend_c1 = 0;
     bool pending = false;
     cudaEvent_t ev[5]{};
+    // the captured Jacobian build of pcc_jacobian_device (CUDA graph), for one
+    // set of device pointers
+    cudaGraphExec_t build_graph = nullptr;
+    const void* graph_key[3] = {nullptr, nullptr, nullptr};
     pcc::MarchLaunchInfo last_launch{};
 };
 

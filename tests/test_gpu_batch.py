@@ -147,3 +147,25 @@ def test_jacobian_columns_device_blocks(engine):
         s.jacobian_columns_device(din.data_ptr(), dout.data_ptr(), c0, c1, cols.data_ptr())
         s.sync()
         assert np.array_equal(cols.cpu().numpy().reshape(c1 - c0, nn).T, J[:, c0:c1])
+
+
+def test_jacobian_device_graph_replays(engine):
+    """pcc_jacobian_device captures its build into a CUDA graph on the first
+    call for a set of pointers and replays it afterwards: every replay gives
+    the bits of pcc_jacobian, with valid timings and counters; new pointers
+    are captured anew."""
+    import torch
+
+    d = load_case("c1_fixture")
+    s = _solve(engine, d["cfg"])
+    nn = s.nn
+    out0 = s.shoot(d["in0"])
+    J = s.jacobian(d["in0"], out0)
+    din = torch.tensor(d["in0"], dtype=torch.float64, device="cuda")
+    dout = torch.tensor(out0, dtype=torch.float64, device="cuda")
+    for k in range(3):
+        dJ = torch.full((nn, nn), float("nan"), dtype=torch.float64, device="cuda")
+        s.jacobian_device(din.data_ptr(), dout.data_ptr(), dJ.data_ptr())
+        st = s.sync()
+        assert np.array_equal(dJ.cpu().numpy(), J), k
+        assert st["ms_sweep"] > 0 and st["rhs_evals"] > 0 and st["shoots"] == nn
