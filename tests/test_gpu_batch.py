@@ -163,9 +163,12 @@ def test_jacobian_device_graph_replays(engine):
     J = s.jacobian(d["in0"], out0)
     din = torch.tensor(d["in0"], dtype=torch.float64, device="cuda")
     dout = torch.tensor(out0, dtype=torch.float64, device="cuda")
-    for k in range(3):
-        dJ = torch.full((nn, nn), float("nan"), dtype=torch.float64, device="cuda")
-        s.jacobian_device(din.data_ptr(), dout.data_ptr(), dJ.data_ptr())
+    dJ = torch.empty((nn, nn), dtype=torch.float64, device="cuda")
+    dJ2 = torch.empty((nn, nn), dtype=torch.float64, device="cuda")
+    for k, target in enumerate([dJ, dJ, dJ, dJ2]):  # capture, two replays, capture anew
+        target.fill_(float("nan"))
+        torch.cuda.synchronize()
+        s.jacobian_device(din.data_ptr(), dout.data_ptr(), target.data_ptr())
         st = s.sync()
-        assert np.array_equal(dJ.cpu().numpy(), J), k
+        assert np.array_equal(target.cpu().numpy(), J), k
         assert st["ms_sweep"] > 0 and st["rhs_evals"] > 0 and st["shoots"] == nn
