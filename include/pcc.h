@@ -315,6 +315,16 @@ pcc_status pcc_expansions_static(pcc_ctx* ctx, int ntau, double dim, double delt
  * log2(ntau_out/ntau_in) times; powers of two, 4 <= ntau_in <= ntau_out <= 4096. */
 pcc_status pcc_resample_fields(pcc_ctx* ctx, int ntau_in, int ntau_out, int count, const double* in, double* out);
 
+/* The IRK march kernel's transform schedule for (Ntau, stages) on the
+ * context's device, picked by this library's autotuner (no counterpart in the
+ * reference): 1 = the independent transforms of an RHS evaluation run in
+ * pairs, 0 = one at a time.  The first solve of a shape times both on a short
+ * single-RHS probe and caches the choice ($PCC_AUTOTUNE_CACHE, default
+ * ~/.cache/pcc_b200/autotune.txt; $PCC_AUTOTUNE=0 keeps pairs); this call
+ * tunes now if needed.  ms_pair/ms_single: probe times, 0 when read from the
+ * cache. */
+pcc_status pcc_march_tuning(pcc_ctx* ctx, int ntau, int stages, int* pair, double* ms_pair, double* ms_single);
+
 /* Replaces the solve's x-grid (NewtonSolver::generateGrid output) by grid,
  * NLeft + NRight + 1 points, as ShootingSolver::shoot accepts any gridX. */
 pcc_status pcc_solve_set_grid(pcc_solve* s, const double* grid);

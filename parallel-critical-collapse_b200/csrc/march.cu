@@ -1,27 +1,34 @@
 // march.cu -- instantiations of the persistent IRK march kernel for one Ntau
-// (PCC_MARCH_N, set by the build: one translation unit per Ntau so that the
-// fifteen shapes compile in parallel) and, with PCC_MARCH_DISPATCH, the
-// launcher that selects among them.
+// and one transform schedule (PCC_MARCH_N, PCC_MARCH_PAIR, set by the build:
+// one translation unit each so that the shapes compile in parallel) and, with
+// PCC_MARCH_DISPATCH, the launcher that selects among them and the autotuner
+// that picks the schedule per (device, Ntau, stages).
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
 #include "pcc_internal.h"
 
 namespace pcc {
 
 namespace {
 
-template <int N, int S>
+template <int N, int S, bool PAIR>
 constexpr int min_blocks()
 {
     // The radix-8 RHS needs ~230 registers per thread without spilling, so a
     // 128-thread CTA reaches two resident CTAs per SM and wider CTAs one.
-    constexpr int nt = MarchShape<N, S>::NT;
+    constexpr int nt = MarchShape<N, S, PAIR>::NT;
     return nt <= 128 ? 2 : 1;
 }
 
-template <int N, int S>
+template <int N, int S, bool PAIR>
 cudaError_t launch_shape(const MarchParams& P, int max_ctas, cudaStream_t st, MarchLaunchInfo* info)
 {
-    using K = MarchShape<N, S>;
-    auto kern = march_kernel<N, S, min_blocks<N, S>()>;
+    using K = MarchShape<N, S, PAIR>;
+    auto kern = march_kernel<N, S, min_blocks<N, S, PAIR>(), PAIR>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0;
@@ -45,13 +52,13 @@ cudaError_t launch_shape(const MarchParams& P, int max_ctas, cudaStream_t st, Ma
     return cudaGetLastError();
 }
 
-template <int N>
+template <int N, bool PAIR>
 cudaError_t launch_n(int stages, const MarchParams& P, int max_ctas, cudaStream_t st, MarchLaunchInfo* info)
 {
     switch (stages) {
-        case 1: return launch_shape<N, 1>(P, max_ctas, st, info);
-        case 2: return launch_shape<N, 2>(P, max_ctas, st, info);
-        case 3: return launch_shape<N, 3>(P, max_ctas, st, info);
+        case 1: return launch_shape<N, 1, PAIR>(P, max_ctas, st, info);
+        case 2: return launch_shape<N, 2, PAIR>(P, max_ctas, st, info);
+        case 3: return launch_shape<N, 3, PAIR>(P, max_ctas, st, info);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -61,10 +68,12 @@ cudaError_t launch_n(int stages, const MarchParams& P, int max_ctas, cudaStream_
 #ifdef PCC_MARCH_N
 #define PCC_CAT2(a, b) a##b
 #define PCC_CAT(a, b) PCC_CAT2(a, b)
-cudaError_t PCC_CAT(launch_march_n, PCC_MARCH_N)(int stages, const MarchParams& P, int max_ctas, cudaStream_t st,
-                                                 MarchLaunchInfo* info)
+#define PCC_CAT4(a, b, c, d) PCC_CAT(PCC_CAT(a, b), PCC_CAT(c, d))
+cudaError_t PCC_CAT4(launch_march_n, PCC_MARCH_N, _p, PCC_MARCH_PAIR)(int stages, const MarchParams& P,
+                                                                     int max_ctas, cudaStream_t st,
+                                                                     MarchLaunchInfo* info)
 {
-    return launch_n<PCC_MARCH_N>(stages, P, max_ctas, st, info);
+    return launch_n<PCC_MARCH_N, PCC_MARCH_PAIR != 0>(stages, P, max_ctas, st, info);
 }
 #endif
 
@@ -100,11 +109,15 @@ cudaError_t launch_march_batch(const BatchParams& B, int max_ctas, cudaStream_t 
 #endif
 
 #ifdef PCC_MARCH_DISPATCH
-cudaError_t launch_march_n128(int, const MarchParams&, int, cudaStream_t, MarchLaunchInfo*);
-cudaError_t launch_march_n256(int, const MarchParams&, int, cudaStream_t, MarchLaunchInfo*);
-cudaError_t launch_march_n512(int, const MarchParams&, int, cudaStream_t, MarchLaunchInfo*);
-cudaError_t launch_march_n1024(int, const MarchParams&, int, cudaStream_t, MarchLaunchInfo*);
-cudaError_t launch_march_n2048(int, const MarchParams&, int, cudaStream_t, MarchLaunchInfo*);
+#define PCC_DECL(n)                                                                                      \
+    cudaError_t launch_march_n##n##_p0(int, const MarchParams&, int, cudaStream_t, MarchLaunchInfo*);    \
+    cudaError_t launch_march_n##n##_p1(int, const MarchParams&, int, cudaStream_t, MarchLaunchInfo*);
+PCC_DECL(128)
+PCC_DECL(256)
+PCC_DECL(512)
+PCC_DECL(1024)
+PCC_DECL(2048)
+#undef PCC_DECL
 
 bool march_supported(int ntau, int stages)
 {
@@ -112,17 +125,129 @@ bool march_supported(int ntau, int stages)
     return n_ok && stages >= 1 && stages <= 3;
 }
 
+namespace {
+
+// Autotuned transform schedule per (device, Ntau, stages): 1 paired, 0 single.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, MarchTuning> g_tuned;
+
+cudaError_t launch_variant(int ntau, int stages, const MarchParams& P, int max_ctas, cudaStream_t st,
+                           MarchLaunchInfo* info, bool pair)
+{
+#define PCC_CASE(n)                                                                                           \
+    case n:                                                                                                   \
+        return pair ? launch_march_n##n##_p1(stages, P, max_ctas, st, info)                                   \
+                    : launch_march_n##n##_p0(stages, P, max_ctas, st, info);
+    switch (ntau) {
+        PCC_CASE(128)
+        PCC_CASE(256)
+        PCC_CASE(512)
+        PCC_CASE(1024)
+        PCC_CASE(2048)
+        default: return cudaErrorInvalidValue;
+    }
+#undef PCC_CASE
+}
+
+}  // namespace
+
+bool march_tuning(int device, int ntau, int stages, MarchTuning* out)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(std::make_tuple(device, ntau, stages));
+    if (it == g_tuned.end()) return false;
+    if (out) *out = it->second;
+    return true;
+}
+
+void march_set_tuning(int device, int ntau, int stages, const MarchTuning& t)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[std::make_tuple(device, ntau, stages)] = t;
+}
+
 cudaError_t launch_march(int ntau, int stages, const MarchParams& P, int max_ctas, cudaStream_t st,
                          MarchLaunchInfo* info)
 {
-    switch (ntau) {
-        case 128: return launch_march_n128(stages, P, max_ctas, st, info);
-        case 256: return launch_march_n256(stages, P, max_ctas, st, info);
-        case 512: return launch_march_n512(stages, P, max_ctas, st, info);
-        case 1024: return launch_march_n1024(stages, P, max_ctas, st, info);
-        case 2048: return launch_march_n2048(stages, P, max_ctas, st, info);
-        default: return cudaErrorInvalidValue;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    MarchTuning t{};
+    const bool pair = march_tuning(dev, ntau, stages, &t) ? t.pair != 0 : true;  // untuned: paired
+    return launch_variant(ntau, stages, P, max_ctas, st, info, pair);
+}
+
+// Times both transform schedules on the kernel's single-RHS mode: items
+// marching no step, one RHS evaluation each, over four waves of sweep slots,
+// from a smooth synthetic state (Delta = 3.4 in its slot).  The faster one is
+// recorded for (device, Ntau, stages).  Allocates and frees its own buffers.
+cudaError_t march_autotune(int ntau, int stages, const double2* tw, cudaStream_t st, MarchTuning* out)
+{
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const int items = 4 * 2 * sms * (ntau >= 1024 ? 1 : 1024 / ntau);
+    std::vector<double> y((size_t)items * ntau, 0.0), xs(items, 0.5);
+    for (int i = 0; i < items; ++i) {
+        double* s = &y[(size_t)i * ntau];
+        for (int m = 0; m < ntau / 2; ++m) s[2 * m] = 1e-2 * std::exp(-0.5 * m) * (1.0 + 0.01 * (i % 7));
+        s[4] = 3.4;  // Re Y[2]: the echoing period
     }
+    double *d_y = nullptr, *d_out = nullptr, *d_x = nullptr;
+    int* d_cnt = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    const size_t by = y.size() * sizeof(double);
+    e = cudaMalloc(&d_y, by);
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, by);
+    if (e == cudaSuccess) e = cudaMalloc(&d_x, items * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_cnt, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_y, y.data(), by, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_x, xs.data(), items * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    double ms[2] = {0.0, 0.0};
+    for (int v = 0; v < 2 && e == cudaSuccess; ++v) {
+        MarchParams P{};
+        P.n_items = items;
+        P.mode = 1;
+        P.yinit = d_y;
+        P.yfinal = d_out;
+        P.dim = 4.0;
+        P.dim_m2_cubed = 8.0;
+        P.prec = 1e-15;
+        P.max_its = 100;
+        P.stages = stages;
+        P.twN = tw;
+        P.x_in = d_x;
+        P.work_counter = d_cnt;
+        float best = 1e30f;
+        for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {  // one warm-up, best of three
+            e = cudaMemsetAsync(d_cnt, 0, sizeof(int), st);
+            if (e == cudaSuccess) e = cudaEventRecord(a, st);
+            if (e == cudaSuccess) e = launch_variant(ntau, stages, P, 0, st, nullptr, v == 1);
+            if (e == cudaSuccess) e = cudaEventRecord(b, st);
+            if (e == cudaSuccess) e = cudaEventSynchronize(b);
+            float t = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+            if (rep > 0 && t < best) best = t;
+        }
+        ms[v] = best;
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    cudaFree(d_y);
+    cudaFree(d_out);
+    cudaFree(d_x);
+    cudaFree(d_cnt);
+    if (e != cudaSuccess) return e;
+    MarchTuning t{};
+    t.pair = ms[1] <= ms[0] ? 1 : 0;
+    t.ms_single = ms[0];
+    t.ms_pair = ms[1];
+    march_set_tuning(dev, ntau, stages, t);
+    if (out) *out = t;
+    return cudaSuccess;
 }
 #endif
 

@@ -69,7 +69,7 @@ struct MarchParams {
     double* snap;                  // [slot][N] states at the start of the steps snap_slot marks
 };
 
-template <int N, int S>
+template <int N, int S, bool PAIR = true>
 struct MarchShape {
     static constexpr int M = N / 2;
     static constexpr int Q = N / 4;
@@ -87,8 +87,9 @@ struct MarchShape {
     static constexpr int UV = S * M;                          // U and V per stage (doubles -> M double2)
     static constexpr int MISC = (S + NW + 1) / 2 + 2;          // lam, red, item, zero (in double2)
     // paired transforms (dft_m2) need a second set of exchange pairs; shapes
-    // whose shared memory would not fit keep single transforms
-    static constexpr bool DUAL = (size_t)SPC * (2 * EXA + YS + YK + UV + MISC) * 16 <= 200 * 1024;
+    // whose shared memory would not fit keep single transforms, and PAIR =
+    // false (a variant the autotuner may pick) never pairs
+    static constexpr bool DUAL = PAIR && (size_t)SPC * (2 * EXA + YS + YK + UV + MISC) * 16 <= 200 * 1024;
     static constexpr int EX = DUAL ? 2 * EXA : EXA;           // exchange double2s
     static constexpr int PER_SWEEP = EX + YS + YK + UV + MISC; // double2 per sweep
     static constexpr size_t SMEM = (size_t)SPC * PER_SWEEP * sizeof(double2);
@@ -634,9 +635,9 @@ __device__ __forceinline__ double sweep_sum(double x, double* red, int lt, const
 
 // ------------------------------------------------------------ sweep slot
 // Shared-memory partition and thread roles of one sweep slot of a CTA.
-template <int N, int S>
+template <int N, int S, bool PAIR = true>
 struct Slot {
-    using K = MarchShape<N, S>;
+    using K = MarchShape<N, S, PAIR>;
     double2* ex;    // [S][2][MP]; the stage RHS lands in one buffer of each pair
     double2* ys;    // [8][TG] slot-indexed y
     double2* ykm;   // this group's stage values [8][TG]
@@ -713,10 +714,10 @@ struct Slot {
 };
 
 // state -> slots: y (group 0) and every stage value (its own group)
-template <int N, int S>
-__device__ __forceinline__ void load_state(const Slot<N, S>& sl, const double* __restrict__ yin)
+template <int N, int S, bool PAIR>
+__device__ __forceinline__ void load_state(const Slot<N, S, PAIR>& sl, const double* __restrict__ yin)
 {
-    constexpr int TG = MarchShape<N, S>::TG;
+    constexpr int TG = MarchShape<N, S, PAIR>::TG;
     if (sl.active) {
 #pragma unroll
         for (int sg = 0; sg < 8; ++sg) {
@@ -763,12 +764,12 @@ struct ParamScalars {
 // The caller has loaded the state (load_state) and synchronised.  Outputs
 // are addressed through sc only where they are written, so that no output
 // pointer stays live across the march.
-template <int N, int S, class SC>
-__device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S>& sl, double k0, int side, int item,
+template <int N, int S, bool PAIR, class SC>
+__device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S, PAIR>& sl, double k0, int side, int item,
                                            unsigned long long& n_its, unsigned long long& n_steps)
 {
     const int mode = sc.mode();
-    using K = MarchShape<N, S>;
+    using K = MarchShape<N, S, PAIR>;
     constexpr int TG = K::TG, STP = K::STP;
     const int s = sl.s, t = sl.t;
     const bool active = sl.active;
@@ -938,13 +939,13 @@ __device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S>& sl, d
 }
 
 // ------------------------------------------------------------------ kernel
-template <int N, int S, int MINB>
-__global__ void __launch_bounds__(MarchShape<N, S>::NT, MINB) march_kernel(MarchParams P)
+template <int N, int S, int MINB, bool PAIR>
+__global__ void __launch_bounds__(MarchShape<N, S, PAIR>::NT, MINB) march_kernel(MarchParams P)
 {
-    using K = MarchShape<N, S>;
+    using K = MarchShape<N, S, PAIR>;
     constexpr int TG = K::TG;
     extern __shared__ double2 smem[];
-    const Slot<N, S> sl(smem, threadIdx.x);
+    const Slot<N, S, PAIR> sl(smem, threadIdx.x);
     if (sl.lt == 0) *sl.zero = 0;
     const ParamScalars sc{P};
     unsigned long long n_its = 0, n_steps = 0;

@@ -9,6 +9,10 @@
 // Column index Nnewton denotes the unperturbed base shoot.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <filesystem>
+#include <fstream>
+#include <sstream>
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -326,6 +330,59 @@ pcc_status collect(pcc_solve* s, int c0, int c1, pcc_stats* stats)
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// The autotuner's cache: one line per (device name, Ntau, stages) with the
+// chosen schedule and the probe times.  $PCC_AUTOTUNE_CACHE, else
+// ~/.cache/pcc_b200/autotune.txt; $PCC_AUTOTUNE=0 disables tuning (paired
+// transforms everywhere).
+std::string autotune_cache_path()
+{
+    if (const char* p = std::getenv("PCC_AUTOTUNE_CACHE")) return p;
+    const char* home = std::getenv("HOME");
+    return std::string(home ? home : ".") + "/.cache/pcc_b200/autotune.txt";
+}
+
+std::mutex g_autotune_mu;
+
+// Makes sure the march kernel's transform schedule for (Ntau, stages) is
+// chosen on the context's device: from the cache file, else by timing both
+// schedules now (march_autotune) and appending the result to the cache.
+void ensure_march_tuned(pcc_ctx* ctx, int ntau, int stages, const double2* d_tw, cudaStream_t st)
+{
+    std::lock_guard<std::mutex> lk(g_autotune_mu);
+    if (march_tuning(ctx->device, ntau, stages, nullptr)) return;
+    if (const char* off = std::getenv("PCC_AUTOTUNE"))
+        if (std::string(off) == "0") return;
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess) return;
+    const std::string name = prop.name;
+    const std::string path = autotune_cache_path();
+    {
+        std::ifstream f(path);
+        std::string line;
+        while (std::getline(f, line)) {
+            std::istringstream is(line);
+            std::string dev;
+            int n = 0, s = 0, pair = 1;
+            double mp = 0, ms = 0;
+            if (!std::getline(is, dev, '\t')) continue;
+            if (!(is >> n >> s >> pair >> mp >> ms)) continue;
+            if (dev == name && n == ntau && s == stages) {
+                march_set_tuning(ctx->device, ntau, stages, MarchTuning{pair, 0.0, 0.0});
+                return;
+            }
+        }
+    }
+    MarchTuning t{};
+    if (march_autotune(ntau, stages, d_tw, st, &t) != cudaSuccess) {
+        cudaGetLastError();  // keep the default schedule
+        return;
+    }
+    std::error_code ec;
+    std::filesystem::create_directories(std::filesystem::path(path).parent_path(), ec);
+    std::ofstream out(path, std::ios::app);
+    if (out) out << name << '\t' << ntau << ' ' << stages << ' ' << t.pair << ' ' << t.ms_pair << ' ' << t.ms_single << '\n';
+}
+
 // One persistent launch over the sweeps of columns [0, ncols[i]) of every
 // solve in v, with the context's own tables.
 pcc_status enqueue_batch_march(pcc_ctx* ctx, const std::vector<pcc_solve*>& v, const std::vector<int>& ncols,
@@ -503,6 +560,8 @@ pcc_status solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, cudaStream_t a
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the host tables may go once copied
     for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&s->ev[i]);
     if (e != cudaSuccess) return cleanup(PCC_ERR_CUDA, cudaGetErrorString(e));
+    // serving runs the batch kernel only, and must not synchronise the device
+    if (!alloc_st) ensure_march_tuned(ctx, n, s->stages, s->d_tw, st);
     if (registered) ctx->solves.push_back(s);
     *out = s;
     return PCC_OK;
@@ -1333,6 +1392,28 @@ pcc_status pcc_resample_fields(pcc_ctx* ctx, int ntau_in, int ntau_out, int coun
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(buf);
     if (e != cudaSuccess) return fail(ctx, PCC_ERR_CUDA, cudaGetErrorString(e));
+    return PCC_OK;
+}
+
+pcc_status pcc_march_tuning(pcc_ctx* ctx, int ntau, int stages, int* pair, double* ms_pair, double* ms_single)
+{
+    if (!ctx || !pair) return PCC_ERR_INVALID_ARG;
+    if (!march_supported(ntau, stages)) return fail(ctx, PCC_ERR_INVALID_ARG, "Ntau 128..2048, 1..3 stages");
+    PCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    MarchTuning t{};
+    if (!march_tuning(ctx->device, ntau, stages, &t)) {
+        double2* d_tw = nullptr;
+        const std::vector<double2> tw = twiddles(ntau);
+        PCC_CUDA(ctx, cudaMalloc(&d_tw, ntau * sizeof(double2)));
+        cudaError_t e = cudaMemcpy(d_tw, tw.data(), ntau * sizeof(double2), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) ensure_march_tuned(ctx, ntau, stages, d_tw, ctx->stream);
+        cudaFree(d_tw);
+        if (e != cudaSuccess) return fail(ctx, PCC_ERR_CUDA, cudaGetErrorString(e));
+        if (!march_tuning(ctx->device, ntau, stages, &t)) t = MarchTuning{1, 0.0, 0.0};  // tuning disabled
+    }
+    *pair = t.pair;
+    if (ms_pair) *ms_pair = t.ms_pair;
+    if (ms_single) *ms_single = t.ms_single;
     return PCC_OK;
 }
 

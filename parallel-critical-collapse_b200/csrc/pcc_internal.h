@@ -43,6 +43,18 @@ cudaError_t launch_march(int ntau, int stages, const MarchParams& P, int max_cta
                          MarchLaunchInfo* info);
 bool march_supported(int ntau, int stages);
 
+// The autotuned transform schedule of the march for one (device, Ntau,
+// stages): paired transforms (dft_m2) or single ones, with the probe times.
+struct MarchTuning {
+    int pair;          // 1 paired, 0 single
+    double ms_pair;    // probe time of each schedule (ms), 0 when set from a cache
+    double ms_single;
+};
+bool march_tuning(int device, int ntau, int stages, MarchTuning* out);
+void march_set_tuning(int device, int ntau, int stages, const MarchTuning& t);
+// Times both schedules on the current device and records the faster one.
+cudaError_t march_autotune(int ntau, int stages, const double2* tw, cudaStream_t st, MarchTuning* out);
+
 // Sweeps of several solves in one persistent launch (march_batch_kernel):
 // Ntau in {128, 256, 512, 1024} with 2 stages.  B.cls_counter must be zero.
 cudaError_t launch_march_batch(const BatchParams& B, int max_ctas, cudaStream_t st, MarchLaunchInfo* info);

@@ -37,7 +37,8 @@ EXPORTS = ["pcc_ctx_create", "pcc_ctx_destroy", "pcc_status_string", "pcc_last_e
            "pcc_unpack_fields", "pcc_expansions", "pcc_solve_set_grid", "pcc_dft", "pcc_expansions_static",
            "pcc_jacobian_batch", "pcc_newton_begin", "pcc_newton_iterate", "pcc_newton_result",
            "pcc_newton_solve", "pcc_serve_start", "pcc_submit", "pcc_poll", "pcc_wait", "pcc_serve_stats",
-           "pcc_serve_stop", "pcc_resample_fields", "pcc_shoot_debug", "pcc_jacobian_columns_device"]
+           "pcc_serve_stop", "pcc_resample_fields", "pcc_shoot_debug", "pcc_jacobian_columns_device",
+           "pcc_march_tuning"]
 
 NEWTON_CODES = ["RUNNING", "CONVERGED", "STOPPED", "MAX_ITER", "IRK_FAILED", "DELTA_MISMATCH", "SINGULAR"]
 
@@ -181,6 +182,7 @@ def load(path=None):
     L.pcc_resample_fields.argtypes = [vp, ci, ci, ci, _D, _D]
     L.pcc_shoot_debug.argtypes = [vp, _D, _D, ci, ci, _I, _I, _D, ctypes.POINTER(Stats)]
     L.pcc_jacobian_columns_device.argtypes = [vp, vp, vp, ci, ci, vp]
+    L.pcc_march_tuning.argtypes = [vp, ci, ci, _I, _D, _D]
     for name in EXPORTS:
         if name not in ("pcc_status_string", "pcc_last_error"):
             getattr(L, name).restype = ci
@@ -377,6 +379,14 @@ class Engine:
 
     def serve_stop(self):
         self._check(self.lib.pcc_serve_stop(self.ctx))
+
+    def march_tuning(self, ntau, stages=2):
+        """The autotuned transform schedule: {'pair': 0/1, 'ms_pair', 'ms_single'}."""
+        pair = ctypes.c_int(0)
+        mp, ms = ctypes.c_double(0), ctypes.c_double(0)
+        self._check(self.lib.pcc_march_tuning(self.ctx, ntau, stages, ctypes.byref(pair), ctypes.byref(mp),
+                                              ctypes.byref(ms)))
+        return {"pair": pair.value, "ms_pair": mp.value, "ms_single": ms.value}
 
     def fp64_peak_tflops(self):
         v = ctypes.c_double(0)
