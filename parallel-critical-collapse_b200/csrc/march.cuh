@@ -57,7 +57,7 @@ struct MarchParams {
     double a[3][3], b[3], c[3];
     int predictor;                     // 1: stage iteration starts from the extrapolated collocation polynomial
     double lq[3][3];                   // int_0^theta l_j = sum_k lq[j][k] theta^(k+1) (Lagrange basis on c)
-    const double2* __restrict__ twN;   // exp(+2 pi i k/N), k < N
+    const double2* __restrict__ twN;   // exp(+2 pi i k/N), k < N, then the pass tables (march_twiddle_count)
     const double* __restrict__ x_in;   // [item] (modes 1 and 2)
     const double* __restrict__ x_out;  // [item] (mode 2)
     int* work_counter;
@@ -152,6 +152,23 @@ __device__ __forceinline__ void dft8(double2 (&a)[8])
     a[6] = t;
 }
 
+// Per-pass twiddle tables.  The twiddle buffer of a march holds the N = 2M
+// point twiddles exp(+2 pi i k/N) followed by one table per Stockham pass of
+// span NS = 8, 64, 512 (< M) of the length-M transforms: the pass of radix
+// R = min(8, M/NS) stores exp(+2 pi i r k/(NS R)) at (r-1) NS + k, r < R,
+// k < NS.  The threads of a warp take consecutive k, so a pass's twiddle
+// loads are contiguous; read from the point table they would be strided by
+// 2 r k entries (up to one cache line per thread).
+__host__ __device__ constexpr int pass_radix(int M, int NS) { return M / NS < 8 ? M / NS : 8; }
+__host__ __device__ constexpr int pass_table_offset(int M, int NS)
+{
+    int off = 0;
+    for (int s = 8; s < NS; s *= 8) off += (pass_radix(M, s) - 1) * s;
+    return off;
+}
+// double2 entries of the twiddle buffer of a march over Ntau = N
+__host__ __device__ constexpr int march_twiddle_count(int N) { return N + pass_table_offset(N / 2, N / 2); }
+
 // Twiddles of one Stockham pass (radix R, span NS) for thread t: element r of
 // butterfly u = t + TG u' is multiplied by w_M^{SG r k M/(NS R)}, k = j mod NS.
 // Fetched separately so that the loads can be issued before the barrier that
@@ -159,14 +176,15 @@ __device__ __forceinline__ void dft8(double2 (&a)[8])
 template <int M, int TG, int R, int NS, int SG>
 __device__ __forceinline__ void fetch_twiddles(double2 (&w)[7], int t, const double2* __restrict__ twN, int zoff)
 {
+    static_assert(R == pass_radix(M, NS), "pass table radix");
     constexpr int B = 8 / R;
+    const double2* __restrict__ tab = twN + 2 * M + pass_table_offset(M, NS);
 #pragma unroll
     for (int u = 0; u < B; ++u) {
         const int k = (t + TG * u) & (NS - 1);
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-            const int idx = r * k * (M / (NS * R));  // exponent of w_M, < M
-            double2 x = __ldg(&twN[2 * idx + zoff]);
+            double2 x = __ldg(&tab[(r - 1) * NS + k + zoff]);
             if (SG < 0) x.y = -x.y;
             w[u * (R - 1) + (r - 1)] = x;
         }

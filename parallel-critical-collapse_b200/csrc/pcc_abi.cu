@@ -108,14 +108,28 @@ void lagrange_integrals(int stages, const double c[3], double lq[3][3])
     }
 }
 
-// exp(+2 pi i k/n), k < n, rounded from long-double trigonometry
+// exp(+2 pi i k/n), k < n, rounded from long-double trigonometry, followed
+// for the march's sizes by its per-pass tables (march_twiddle_count(n)
+// entries in all), whose entries are copies of point twiddles: the
+// exponent r k/(NS R) of a length-M pass is 2 r k M/(NS R) / n.
+int twiddle_count(int n) { return march_supported(n, 1) ? march_twiddle_count(n) : n; }
+
 std::vector<double2> twiddles(int n)
 {
-    std::vector<double2> tw(n);
+    std::vector<double2> tw(twiddle_count(n));
     const long double two_pi = 6.283185307179586476925286766559005768L;
     for (int k = 0; k < n; ++k) {
         const long double a = two_pi * (long double)k / (long double)n;
         tw[k] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    if ((int)tw.size() > n) {
+        const int M = n / 2;
+        for (int ns = 8; ns < M; ns *= 8) {
+            const int R = pass_radix(M, ns);
+            double2* tab = tw.data() + n + pass_table_offset(M, ns);
+            for (int r = 1; r < R; ++r)
+                for (int k = 0; k < ns; ++k) tab[(r - 1) * ns + k] = tw[2 * (r * k * (M / (ns * R)))];
+        }
     }
     return tw;
 }
@@ -488,7 +502,7 @@ size_t solve_footprint(const pcc_solve_desc& d, int sms)
 {
     const size_t n = d.ntau, nn = 3 * n / 4, cols = nn + 1, ngrid = (size_t)d.nl + d.nr + 1;
     const size_t dbl = sizeof(double), in = sizeof(int);
-    return ngrid * dbl + n * sizeof(double2) + 2 * nn * dbl + nn * nn * dbl + 2 * (2 * cols * n * dbl) +
+    return ngrid * dbl + twiddle_count(n) * sizeof(double2) + 2 * nn * dbl + nn * nn * dbl + 2 * (2 * cols * n * dbl) +
            cols * nn * dbl + 2 * (2 * cols * in) + cols * in + 4 * in + 4 * sizeof(unsigned long long) +
            (size_t)2 * sms * kBoundaryArrays * n * dbl + 2 * cols * in + 4 * cols * dbl + 2 * cols * in +
            sizeof(NewtonDev) + 3 * nn * dbl + nn * in + 2 * in + lu_mixed_work_bytes((int)nn) + in;
@@ -525,7 +539,7 @@ pcc_status solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, cudaStream_t a
         s->footprint += (bytes);                                                                             \
     } while (0)
     ALLOC(s->d_grid, s->ngrid * sizeof(double));
-    ALLOC(s->d_tw, n * sizeof(double2));
+    ALLOC(s->d_tw, twiddle_count(n) * sizeof(double2));
     ALLOC(s->d_in0, nn * sizeof(double));
     ALLOC(s->d_out0, nn * sizeof(double));
     ALLOC(s->d_J, (size_t)nn * nn * sizeof(double));
@@ -552,7 +566,8 @@ pcc_status solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, cudaStream_t a
 #undef ALLOC
     cudaStream_t st = alloc_st ? alloc_st : ctx->stream;
     s->tw_host = twiddles(n);
-    cudaError_t e = cudaMemcpyAsync(s->d_tw, s->tw_host.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st);
+    cudaError_t e = cudaMemcpyAsync(s->d_tw, s->tw_host.data(), s->tw_host.size() * sizeof(double2),
+                                    cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->d_grid, s->grid.data(), s->ngrid * sizeof(double), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->d_cancel, 0, sizeof(int), st);
@@ -1095,7 +1110,7 @@ static pcc_status single_states(pcc_ctx* ctx, int ntau, double dim, int scheme, 
     };
     if (cudaMalloc(&d_y, yb) != cudaSuccess || cudaMalloc(&d_o, yb) != cudaSuccess ||
         cudaMalloc(&d_x, 2 * count * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&d_tw, ntau * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&d_tw, twiddle_count(ntau) * sizeof(double2)) != cudaSuccess ||
         cudaMalloc(&d_i, (3 * count + 4) * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&d_c, 4 * sizeof(unsigned long long)) != cudaSuccess) {
         release();
@@ -1108,7 +1123,7 @@ static pcc_status single_states(pcc_ctx* ctx, int ntau, double dim, int scheme, 
         xs[count + i] = x_out ? x_out[i] : 0.0;
     }
     cudaError_t e = cudaMemcpy(d_y, y, yb, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(d_tw, tw.data(), ntau * sizeof(double2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_x, xs.data(), 2 * count * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(d_i, 0, (3 * count + 4) * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(d_c, 0, 4 * sizeof(unsigned long long));
@@ -1404,8 +1419,8 @@ pcc_status pcc_march_tuning(pcc_ctx* ctx, int ntau, int stages, int* pair, doubl
     if (!march_tuning(ctx->device, ntau, stages, &t)) {
         double2* d_tw = nullptr;
         const std::vector<double2> tw = twiddles(ntau);
-        PCC_CUDA(ctx, cudaMalloc(&d_tw, ntau * sizeof(double2)));
-        cudaError_t e = cudaMemcpy(d_tw, tw.data(), ntau * sizeof(double2), cudaMemcpyHostToDevice);
+        PCC_CUDA(ctx, cudaMalloc(&d_tw, tw.size() * sizeof(double2)));
+        cudaError_t e = cudaMemcpy(d_tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) ensure_march_tuned(ctx, ntau, stages, d_tw, ctx->stream);
         cudaFree(d_tw);
         if (e != cudaSuccess) return fail(ctx, PCC_ERR_CUDA, cudaGetErrorString(e));
