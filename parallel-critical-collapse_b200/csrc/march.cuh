@@ -245,9 +245,9 @@ __device__ __forceinline__ void load_std(double2 (&v)[8], const double2* __restr
 // standard register layout.  bufs[0..1] ping-pong; `cur` selects the first
 // buffer written and is advanced so that the next transform never writes a
 // buffer that a lagging thread may still be reading.
-template <int M, int TG, int SG>
+template <int M, int TG, int SG, class SY>
 __device__ __forceinline__ void dft_m(double2 (&v)[8], double2* __restrict__ b0, double2* __restrict__ b1,
-                                      int& cur, int t, const double2* __restrict__ twN, const SweepSync& sy,
+                                      int& cur, int t, const double2* __restrict__ twN, const SY& sy,
                                       bool active, const volatile int* zero)
 {
     constexpr int NP = M == 64 ? 2 : (M <= 512 ? 3 : 4);
@@ -297,11 +297,11 @@ __device__ __forceinline__ void dft_m(double2 (&v)[8], double2* __restrict__ b0,
 // the same arithmetic as two dft_m calls, with one twiddle fetch and one
 // barrier per pass for both and twice the independent work between barriers.
 // v uses the buffer pair (a0, a1), u the pair (c0, c1), both selected by cur.
-template <int M, int TG, int SG>
+template <int M, int TG, int SG, class SY>
 __device__ __forceinline__ void dft_m2(double2 (&v)[8], double2 (&u)[8], double2* __restrict__ a0,
                                        double2* __restrict__ a1, double2* __restrict__ c0,
                                        double2* __restrict__ c1, int& cur, int t, const double2* __restrict__ twN,
-                                       const SweepSync& sy, bool active, const volatile int* zero)
+                                       const SY& sy, bool active, const volatile int* zero)
 {
     constexpr int NP = M == 64 ? 2 : (M <= 512 ? 3 : 4);
     constexpr int RL = M == 64 ? 8 : M == 128 ? 2 : M == 256 ? 4 : M == 512 ? 8 : 2;
@@ -404,12 +404,12 @@ __device__ __forceinline__ int slot_q(int sigma)
 // DUAL: the three pairs of independent transforms (U+iV with F, the last IA2
 // transform with dU+idV, the odd with the even forward transform) run as
 // paired transforms (dft_m2) through the second exchange pair c0/c1.
-template <int N, bool DUAL>
+template <int N, bool DUAL, class SY>
 __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double* __restrict__ uvs, double x,
                                          double dim, double dm2c, double k0, int t, double2* __restrict__ b0,
                                          double2* __restrict__ b1, double2* __restrict__ c0,
                                          double2* __restrict__ c1, int& cur, double* lam_slot,
-                                         const double2* __restrict__ twN, const SweepSync& sy, bool active,
+                                         const double2* __restrict__ twN, const SY& sy, bool active,
                                          const volatile int* zero)
 {
     constexpr int M = N / 2, TG = M / 8;
@@ -631,12 +631,12 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
 }
 
 // ------------------------------------------------------------ sweep reduce
-template <int STP, int NW>
-__device__ __forceinline__ double sweep_sum(double x, double* red, int lt, const SweepSync& sy)
+template <int STP, int NW, class SY>
+__device__ __forceinline__ double sweep_sum(double x, double* red, int lt, const SY& sy)
 {
     constexpr int W = STP < 32 ? STP : 32;
 #pragma unroll
-    for (int o = W / 2; o > 0; o >>= 1) x += __shfl_xor_sync(sy.bar_id == 0 ? sy.mask : 0xffffffffu, x, o, 32);
+    for (int o = W / 2; o > 0; o >>= 1) x += __shfl_xor_sync(sy.mask, x, o, 32);
     if constexpr (NW == 1) {
         return x;
     } else {
@@ -668,9 +668,9 @@ struct Slot {
     double2* c0;  // the second transform's exchange pair (K::DUAL)
     double2* c1;
     int slot_id, lt, s, t;
-    bool active;
-    SweepSync sy;   // the whole sweep: IRK update, reductions, state hand-over
-    SweepSync gsy;  // this stage group only: the transforms of its RHS evaluation
+    bool active;    // a working lane (constant true where the sweep has no padding lanes)
+    SweepSync<(K::STP > 32)> sy;  // the whole sweep: IRK update, reductions, state hand-over
+    SweepSync<(K::TG > 32)> gsy;  // this stage group only: the transforms of its RHS evaluation
 
     __device__ __forceinline__ Slot(double2* smem, int tid)
     {
@@ -678,7 +678,7 @@ struct Slot {
         slot_id = tid / STP;
         lt = tid % STP;
         const int s_raw = lt / TG;
-        active = s_raw < S;
+        active = K::ST == K::STP ? true : s_raw < S;
         s = active ? s_raw : S - 1;
         t = lt % TG;
         if constexpr (STP < 32) {

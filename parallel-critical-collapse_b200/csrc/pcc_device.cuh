@@ -65,19 +65,21 @@ __host__ __device__ __forceinline__ int pad8(int i) { return i + (i >> 3); }
 // then maps 8 consecutive lanes to 8 distinct 16-byte bank groups.
 __host__ __device__ __forceinline__ int swz8(int i) { return i ^ ((i >> 3) & 7); }
 
-// Synchronisation of the threads that march one sweep.  Sweeps of at most 32
-// threads live inside one warp and use __syncwarp on their lane mask; wider
-// sweeps use a named barrier (id >= 1) over their own warps.
+// Synchronisation of a group of threads (a sweep, or one stage group of it).
+// Groups of at most 32 threads live inside one warp and use __syncwarp on
+// their lane mask; wider groups (WIDE, fixed by the kernel's shape at compile
+// time) use a named barrier (id >= 1) over their own warps.
+template <bool WIDE>
 struct SweepSync {
-    unsigned mask;  // lane mask (narrow sweeps)
-    int bar_id;     // named barrier id (wide sweeps), 0 for narrow
-    int nthreads;   // threads taking part (multiple of 32 for wide sweeps)
+    unsigned mask;  // lane mask (all lanes for wide groups)
+    int bar_id;     // named barrier id (wide groups)
+    int nthreads;   // threads taking part (multiple of 32 for wide groups)
     __device__ __forceinline__ void sync() const
     {
-        if (bar_id == 0) {
-            __syncwarp(mask);
-        } else {
+        if constexpr (WIDE) {
             asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
+        } else {
+            __syncwarp(mask);
         }
     }
 };
