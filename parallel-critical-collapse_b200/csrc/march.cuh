@@ -491,18 +491,20 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = make_double2(v[q].x * invM, v[q].y * invM);
     if (active && t == 0) *lam_slot = v[0].x;  // lambda = f_hat[0] (real: imag is exactly 0)
-    // lamIntegrate(f_hat, 0): out_k = f_k / (-i m k0) = i f_k / (m k0); DC and Nyquist -> 0
+    // lamIntegrate(f_hat, 0): out_k = f_k / (-i m k0) = i f_k / (m k0); DC and Nyquist -> 0.
+    // Only thread 0 holds the DC (q = 0) and Nyquist (p = M/2 = 4 TG: q = 4)
+    // entries, so every entry takes the general formula without a branch and
+    // thread 0 overwrites those two afterwards.
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const int p = t + TG * q;
-        const int k = 2 * p;
-        if (p == 0 || k == M) {
-            v[q] = make_double2(0.0, 0.0);
-        } else {
-            const int m = k < M ? k : k - N;
-            const double r = 1.0 / (m * k0);
-            v[q] = make_double2(-v[q].y * r, v[q].x * r);
-        }
+        const int k = 2 * (t + TG * q);
+        const int m = k < M ? k : k - N;
+        const double r = 1.0 / (m * k0);
+        v[q] = make_double2(-v[q].y * r, v[q].x * r);
+    }
+    if (t == 0) {
+        v[0] = make_double2(0.0, 0.0);
+        v[4] = make_double2(0.0, 0.0);
     }
     dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
     double Fr[8];
@@ -515,26 +517,30 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
     dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
     const double lam = *lam_slot;  // written before at least one sweep barrier
     {
-        const double s = k0 * N / 2.0;
-        const double2 qn = cdiv(lam, 0.0, lam * lam - 0.0 * 0.0 + s * s, lam * 0.0 + 0.0 * lam);
-        // out_k = h_k / (lambda - i s) = h_k (lambda + i s) / (lambda^2 + s^2), s = m k0
+        // out_k = h_k / (lambda - i s) = h_k (lambda + i s) / (lambda^2 + s^2), s = m k0,
+        // with the DC and Nyquist rules of lamIntegrate for thread 0's q = 0 and
+        // q = 4 entries applied after the branch-free general formula
+        const double2 h0 = make_double2(v[0].x * invM, v[0].y * invM);
+        const double2 h4 = make_double2(v[4].x * invM, v[4].y * invM);
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            const int p = t + TG * q;
-            const int k = 2 * p;
+            const int k = 2 * (t + TG * q);
+            const int m = k < M ? k : k - N;
             const double2 h = make_double2(v[q].x * invM, v[q].y * invM);
-            if (p == 0) {
-                v[q] = lam != 0.0 ? make_double2(h.x / lam, h.y / lam) : make_double2(0.0, 0.0);
-            } else if (k == M) {
-                v[q] = cmul(qn, h);
-            } else {
-                const int m = k < M ? k : k - N;
-                const double sm = m * k0;
-                const double den = lam * lam + sm * sm;  // |lambda - i s|^2
-                const double r = 1.0 / den;
-                v[q] = den < 1e-28 ? make_double2(0.0, 0.0)
-                                   : make_double2((h.x * lam - h.y * sm) * r, (h.y * lam + h.x * sm) * r);
-            }
+            const double sm = m * k0;
+            const double den = lam * lam + sm * sm;  // |lambda - i s|^2
+            const double r = 1.0 / den;
+            v[q] = den < 1e-28 ? make_double2(0.0, 0.0)
+                               : make_double2((h.x * lam - h.y * sm) * r, (h.y * lam + h.x * sm) * r);
+        }
+        if (t == 0) {
+            v[0] = lam != 0.0 ? make_double2(h0.x / lam, h0.y / lam) : make_double2(0.0, 0.0);
+            // Nyquist: the reference multiplies h by the complex quotient
+            // (lambda + 0i) / (lambda^2 + s^2 + 0i), s = k0 N/2 (Smith's method in
+            // std::complex division), which is lambda / (lambda^2 + s^2) exactly
+            const double s = k0 * N / 2.0;
+            const double qn = lam / (lam * lam - 0.0 * 0.0 + s * s);
+            v[4] = cmul(make_double2(qn, 0.0), h4);
         }
     }
     // dU + i dV from -i m k0 c on the odd modes
