@@ -514,8 +514,14 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
         Fr[q] = 1.0 / e;                         // e^{-F}, kept for X e^{-F}
         v[q] = make_double2(-(dim - 3.0) * e, 0.0);  // h = -g e^F
     }
+    // lambda (written by thread 0 after the first IA2 transform, two exchange
+    // barriers ago) and the DC and Nyquist factors of the division below,
+    // taken by every thread before the transform so that they stay off the
+    // critical path
+    const double lam = *lam_slot;
+    const double ilam = lam != 0.0 ? 1.0 / lam : 0.0;
+    const double qn = lam / (lam * lam - 0.0 * 0.0 + (k0 * N / 2.0) * (k0 * N / 2.0));
     dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
-    const double lam = *lam_slot;  // written before at least one sweep barrier
     {
         // out_k = h_k / (lambda - i s) = h_k (lambda + i s) / (lambda^2 + s^2), s = m k0,
         // with the DC and Nyquist rules of lamIntegrate for thread 0's q = 0 and
@@ -534,12 +540,7 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
                                : make_double2((h.x * lam - h.y * sm) * r, (h.y * lam + h.x * sm) * r);
         }
         if (t == 0) {
-            v[0] = lam != 0.0 ? make_double2(h0.x / lam, h0.y / lam) : make_double2(0.0, 0.0);
-            // Nyquist: the reference multiplies h by the complex quotient
-            // (lambda + 0i) / (lambda^2 + s^2 + 0i), s = k0 N/2 (Smith's method in
-            // std::complex division), which is lambda / (lambda^2 + s^2) exactly
-            const double s = k0 * N / 2.0;
-            const double qn = lam / (lam * lam - 0.0 * 0.0 + s * s);
+            v[0] = make_double2(h0.x * ilam, h0.y * ilam);
             v[4] = cmul(make_double2(qn, 0.0), h4);
         }
     }
