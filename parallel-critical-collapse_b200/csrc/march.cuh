@@ -520,6 +520,9 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
     // critical path
     const double lam = *lam_slot;
     const double ilam = lam != 0.0 ? 1.0 / lam : 0.0;
+    // Nyquist: the reference multiplies h by the complex quotient
+    // (lambda + 0i) / (lambda^2 + s^2 + 0i), s = k0 N/2 (Smith's method in
+    // std::complex division), which is lambda / (lambda^2 + s^2) exactly
     const double qn = lam / (lam * lam - 0.0 * 0.0 + (k0 * N / 2.0) * (k0 * N / 2.0));
     dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
     {
