@@ -591,7 +591,8 @@ def run_engine(args, world, rank, local):
                            "ntau": n, "points": cfg["NLeft"] + cfg["NRight"], "columns": nn, "seed": args.seed,
                            "amp": args.amp, "l2": "flushed (256 MB write) before every timed build",
                            "parallelism": f"{world} independent solves, one per GPU",
-                           "sweep_ctas": st_e.sweep_ctas, "wall_s": wall},
+                           "sweep_ctas": st_e.sweep_ctas, "wall_s": wall,
+                           "march_schedule": eng.march_tuning(n, 2)},
                 "clocks": clk, "e2e": e2e, "gpu_launches": 4 * args.steps, "roofline": roofline,
                 "cpu_baseline": cpu, "predictor": predictor, "newton_step": newton, "dscan16": dscan,
                 "serving": serving}

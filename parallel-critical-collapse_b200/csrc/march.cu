@@ -178,8 +178,11 @@ cudaError_t launch_march(int ntau, int stages, const MarchParams& P, int max_cta
 }
 
 // Times both transform schedules on the kernel's single-RHS mode: items
-// marching no step, one RHS evaluation each, over four waves of sweep slots,
-// from a smooth synthetic state (Delta = 3.4 in its slot).  The faster one is
+// marching no step, one RHS evaluation each, over sixteen waves of sweep
+// slots (about half a millisecond at Ntau = 1024), from a smooth synthetic
+// state (Delta = 3.4 in its slot), best of five.  The paired schedule is kept
+// unless the single one is more than 3 % faster: on a full march the two
+// differ by a few per cent, less than a short probe's noise.  The choice is
 // recorded for (device, Ntau, stages).  Allocates and frees its own buffers.
 cudaError_t march_autotune(int ntau, int stages, const double2* tw, cudaStream_t st, MarchTuning* out)
 {
@@ -187,7 +190,7 @@ cudaError_t march_autotune(int ntau, int stages, const double2* tw, cudaStream_t
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    const int items = 4 * 2 * sms * (ntau >= 1024 ? 1 : 1024 / ntau);
+    const int items = 16 * 2 * sms * (ntau >= 1024 ? 1 : 1024 / ntau);
     std::vector<double> y((size_t)items * ntau, 0.0), xs(items, 0.5);
     for (int i = 0; i < items; ++i) {
         double* s = &y[(size_t)i * ntau];
@@ -222,7 +225,7 @@ cudaError_t march_autotune(int ntau, int stages, const double2* tw, cudaStream_t
         P.x_in = d_x;
         P.work_counter = d_cnt;
         float best = 1e30f;
-        for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {  // one warm-up, best of three
+        for (int rep = 0; rep < 6 && e == cudaSuccess; ++rep) {  // one warm-up, best of five
             e = cudaMemsetAsync(d_cnt, 0, sizeof(int), st);
             if (e == cudaSuccess) e = cudaEventRecord(a, st);
             if (e == cudaSuccess) e = launch_variant(ntau, stages, P, 0, st, nullptr, v == 1);
@@ -242,7 +245,7 @@ cudaError_t march_autotune(int ntau, int stages, const double2* tw, cudaStream_t
     cudaFree(d_cnt);
     if (e != cudaSuccess) return e;
     MarchTuning t{};
-    t.pair = ms[1] <= ms[0] ? 1 : 0;
+    t.pair = ms[0] < 0.97 * ms[1] ? 0 : 1;
     t.ms_single = ms[0];
     t.ms_pair = ms[1];
     march_set_tuning(dev, ntau, stages, t);

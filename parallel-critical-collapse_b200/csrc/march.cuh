@@ -966,6 +966,19 @@ __device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S, PAIR>&
 }
 
 // ------------------------------------------------------------------ kernel
+// The item a sweep slot takes for work index w.  A march over (column, side)
+// items (item = 2 column + side, no explicit side map) hands out every
+// right-side sweep first, then the left-side ones; the sweeps and their
+// results are the same in any order.  Measured on the C3 build (1536 sweeps,
+// the same 60.9 M RHS evaluations): 1.187 s against 1.246 s in column order,
+// and 1.192 s with the left sides first.
+__device__ __forceinline__ int march_item_of(int w, const MarchParams& P)
+{
+    if (P.mode != 0 || P.item_side || (P.n_items & 1) || w >= P.n_items) return w;
+    const int h = P.n_items >> 1;
+    return w < h ? 2 * w + 1 : 2 * (w - h);
+}
+
 template <int N, int S, int MINB, bool PAIR>
 __global__ void __launch_bounds__(MarchShape<N, S, PAIR>::NT, MINB) march_kernel(MarchParams P)
 {
@@ -978,7 +991,7 @@ __global__ void __launch_bounds__(MarchShape<N, S, PAIR>::NT, MINB) march_kernel
     unsigned long long n_its = 0, n_steps = 0;
 
     for (;;) {
-        if (sl.lt == 0) *sl.item_slot = atomicAdd(P.work_counter, 1);
+        if (sl.lt == 0) *sl.item_slot = march_item_of(atomicAdd(P.work_counter, 1), P);
         sl.sy.sync();
         const int item = *sl.item_slot;
         sl.sy.sync();

@@ -676,7 +676,12 @@ pcc_status batch_march_items(pcc_ctx* ctx, BatchTables& tab, const std::vector<B
             if (s->d.ntau == n) cls.push_back({(items[i].item & 1) ? s->d.nr : s->d.nl, i});
         }
         if (cls.empty()) continue;
-        std::stable_sort(cls.begin(), cls.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+        // longest sweeps first; among equal lengths the right sides first (the
+        // single-solve march's order, measured faster at C3)
+        std::stable_sort(cls.begin(), cls.end(), [&](const auto& a, const auto& b) {
+            if (a.first != b.first) return a.first > b.first;
+            return (items[a.second].item & 1) > (items[b.second].item & 1);
+        });
         B.cls_ntau[B.n_classes] = n;
         B.cls_begin[B.n_classes] = (int)table.size();
         for (auto& c : cls) table.push_back(make_int2(sidx[c.second], items[c.second].item));

@@ -176,12 +176,13 @@ def test_jacobian_device_graph_replays(engine):
 
 def test_march_autotuner_picks_the_faster_schedule(engine, tmp_path, monkeypatch):
     """The autotuner times paired and single transform schedules on its probe
-    and keeps the faster; the choice lands in the cache file."""
+    and keeps the paired one unless the single one is more than 3 % faster;
+    the choice lands in the cache file."""
     cache = tmp_path / "autotune.txt"
     monkeypatch.setenv("PCC_AUTOTUNE_CACHE", str(cache))
     t = engine.march_tuning(2048, 1)  # a shape no other test builds
     assert t["ms_pair"] > 0 and t["ms_single"] > 0
-    assert t["pair"] == (1 if t["ms_pair"] <= t["ms_single"] else 0)
+    assert t["pair"] == (0 if t["ms_single"] < 0.97 * t["ms_pair"] else 1)
     line = cache.read_text().strip().splitlines()[-1]
     assert line.split("\t")[1].split()[:3] == ["2048", "1", str(t["pair"])]
     assert engine.march_tuning(2048, 1) == t  # remembered
