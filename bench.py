@@ -216,7 +216,7 @@ def gather_columns(local, nn, blocks, world):
 
 
 def run_shard(args, world, rank, local):
-    """One Jacobian split over the ranks (SURVEY-style column sharding): every
+    """One Jacobian split over the ranks by column blocks: every
     rank builds its contiguous block of columns of the same seeded C3 solve
     with one persistent launch, then one all-gather assembles J on every GPU.
     Strong scaling; time = max over ranks of (build + gather) device time."""

@@ -10,7 +10,7 @@ shoots are compared to 1e-10 absolute.  The finite difference with EpsNewton
 = 1e-7 turns that into noise of ~1e-5 of max|J| (oracle against reference:
 2.0e-6), so Jacobians are compared at matrix scale to 2e-5.  With cond(J) ~
 3e6 one Newton step inherits that noise (oracle against reference: Delta
-6e-10 relative); the BASELINE target "Delta to 1e-10" is checked where it is
+6e-10 relative); the parity target "Delta to 1e-10" is checked where it is
 well posed, on the converged Newton solution, which F(x*) = 0 fixes
 independently of Jacobian noise.  The converged free data are determined to
 ||J^-1|| ||dF|| ~ 1.5e5 * 1e-11, i.e. ~5e-8 relative, and are compared to 1e-6.
@@ -187,7 +187,7 @@ def test_newton_update_on_reference_jacobian(engine, precision):
 @pytest.mark.parametrize("precision", [0, 1])
 def test_newton_converged_solution_c1(engine, precision):
     """Newton iterations to the round-off floor; Delta* against the reference's
-    converged Delta* to 1e-10 relative (the BASELINE target), FP64 and mixed."""
+    converged Delta* to 1e-10 relative (the parity target), FP64 and mixed."""
     d = load_case("c1_newton")
     s = _solve(engine, d["cfg"])
     x = d["in0"].copy()

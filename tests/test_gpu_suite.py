@@ -4,7 +4,7 @@ the same suites (tests/golden/make_suite_golden.py); and spectral resampling
 (scripts/create_simulation_data.py:37-58) against the reference script.
 
 Each dimension converges to PrecisionNewton = 1e-12 on both sides, so the
-echoing period agrees to the BASELINE tolerance (1e-10 relative) and the free
+echoing period agrees to the parity tolerance (1e-10 relative) and the free
 data to the Newton noise floor, whatever the seeds were."""
 import json
 import subprocess
