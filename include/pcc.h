@@ -319,7 +319,8 @@ pcc_status pcc_resample_fields(pcc_ctx* ctx, int ntau_in, int ntau_out, int coun
  * context's device, picked by this library's autotuner (no counterpart in the
  * reference): 1 = the independent transforms of an RHS evaluation run in
  * pairs, 0 = one at a time.  The first solve of a shape times both on a short
- * single-RHS probe and caches the choice ($PCC_AUTOTUNE_CACHE, default
+ * single-RHS probe, keeps pairs unless one at a time is more than 3 % faster,
+ * and caches the choice ($PCC_AUTOTUNE_CACHE, default
  * ~/.cache/pcc_b200/autotune.txt; $PCC_AUTOTUNE=0 keeps pairs); this call
  * tunes now if needed.  ms_pair/ms_single: probe times, 0 when read from the
  * cache. */
