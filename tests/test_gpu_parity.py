@@ -42,19 +42,25 @@ def test_rhs_parity(engine, name):
         assert rel_err(dy[k], d["rhs_dy"][k]) < (1e-10 if x > 0.95 else 1e-12), (name, x)
 
 
+def _resample_state(base, ntau):
+    """A state of ntau/2 modes from one of base.size/2 (zero padding or
+    truncation of the spectrum), the Delta slot kept."""
+    y = np.zeros(ntau)
+    m = min(base.size, ntau)
+    y[: m // 2] = base[: m // 2]          # modes 0 .. m/4-1
+    y[ntau - m // 2:] = base[base.size - m // 2:]  # the negative-frequency end
+    y[4] = base[4]  # Delta
+    return y
+
+
 @pytest.mark.parametrize("ntau", [128, 256, 512, 1024, 2048])
 def test_rhs_random_states_vs_oracle(engine, oracle, ntau):
     """Seeded perturbed states at every supported Ntau, including 256 and 2048."""
     d = load_case("c1_fixture")
     cfg = d["cfg"]
     rng = np.random.default_rng(ntau)
-    # resample the C1 boundary state to ntau modes (zero padding / truncation)
     base = d["y_left"]
-    y = np.zeros(ntau)
-    m = min(base.size, ntau)
-    y[: m // 2] = base[: m // 2]          # modes 0 .. m/4-1
-    y[ntau - m // 2:] = base[base.size - m // 2:]  # the negative-frequency end
-    y = y * (1 + 1e-3 * rng.standard_normal(ntau))
+    y = _resample_state(base, ntau) * (1 + 1e-3 * rng.standard_normal(ntau))
     y[4] = base[4]  # Delta
     xs = np.array([0.002, 0.05, 0.3])
     dy = engine.rhs_eval(ntau, cfg["Dim"], np.stack([y] * 3), xs)
@@ -83,6 +89,23 @@ def test_irk_schemes_vs_oracle(engine, oracle, scheme):
     assert conv
     assert rel_err(out[0], ref) < 1e-13
     assert abs(int(its[0]) - k) <= 1
+
+
+@pytest.mark.parametrize("ntau,scheme", [(256, 2), (2048, 2), (2048, 1), (2048, 3), (1024, 1), (1024, 3)])
+def test_irk_step_shapes_vs_oracle(engine, oracle, ntau, scheme):
+    """One IRK step at the kernel shapes the fixtures do not reach: Ntau 256
+    and 2048 (single transforms, 4 to 12 warps per sweep) and the one- and
+    three-stage schemes at Ntau 1024 (paired transforms, up to 6 warps and
+    one CTA per SM), from the C1 step state zero-padded to ntau modes."""
+    d = load_case("c1_fixture")
+    cfg = d["cfg"]
+    y = _resample_state(d["irk_y"][0], ntau)
+    xa, xb = d["irk_x"][0, 0], d["irk_x"][0, 1]
+    out, its = engine.irk_step(ntau, cfg["Dim"], scheme, 1e-15, 100, y[None], [xa], [xb])
+    ref, k, conv = oracle.irk_step(ntau, cfg["Dim"], scheme, 1e-15, 100, y, xa, xb)
+    assert conv
+    assert rel_err(out[0], ref) < 1e-12, (ntau, scheme)
+    assert abs(int(its[0]) - k) <= 1, (ntau, scheme, int(its[0]), k)
 
 
 @pytest.mark.parametrize("name", CASES)
