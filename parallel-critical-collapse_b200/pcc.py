@@ -516,10 +516,10 @@ class Solve:
         sd = np.ascontiguousarray(sides, dtype=np.int32)
         out = np.zeros_like(y)
         st = Stats()
-        self.engine._check(self.lib.pcc_sweep(self.h, y.shape[0], sd.ctypes.data_as(_I), _p(y), _p(out),
-                                              ctypes.byref(st)))
-        if stats is not None:
+        r = self.lib.pcc_sweep(self.h, y.shape[0], sd.ctypes.data_as(_I), _p(y), _p(out), ctypes.byref(st))
+        if stats is not None:  # filled on failure too (the failing sweep and grid index)
             stats.update(st.as_dict())
+        self.engine._check(r)
         return out
 
 

@@ -151,6 +151,32 @@ def test_sweep_vs_oracle(engine, oracle):
     assert abs(st["rhs_evals"] - (e0 + e1)) <= 0.01 * (e0 + e1)
 
 
+def test_sweep_shapes_vs_oracle(engine, oracle):
+    """Left sweeps of the C1 grid from the C1 boundary state zero-padded to
+    more modes.  At Ntau 256 the march converges and matches the oracle; at
+    Ntau 2048 the grid is too coarse for the stiffer spectrum, and both report
+    the IRK failure at the same grid index (the reference exits there)."""
+    import pcc
+
+    d = load_case("c1_fixture")
+    cfg = dict(d["cfg"], Ntau=256)
+    y = _resample_state(d["y_left"], 256)
+    yo, st_o, _, _ = oracle.sweep(cfg, y, True)
+    assert st_o == 0
+    out = _solve(engine, cfg).sweep(y[None], [0])
+    assert np.max(np.abs(out[0] - yo)) < 1e-10
+
+    cfg = dict(d["cfg"], Ntau=2048)
+    y = _resample_state(d["y_left"], 2048)
+    _, st_o, fail_o, _ = oracle.sweep(cfg, y, True)
+    assert st_o != 0
+    st = {}
+    with pytest.raises(pcc.PccError) as e:
+        _solve(engine, cfg).sweep(y[None], [0], stats=st)
+    assert e.value.status == 4
+    assert abs(st["fail_grid_index"] - fail_o) <= 1, (st["fail_grid_index"], fail_o)
+
+
 @pytest.mark.parametrize("name", ["c1_fixture", "c1_perturbed"])
 def test_jacobian_c1(engine, name):
     d = load_case(name)
