@@ -117,6 +117,33 @@ def test_boundary_data_parity(engine, name):
     assert rel_err(yr, d["y_right"]) < 1e-12
 
 
+def _interp_field(f, n):
+    """Spectral (zero-padding) interpolation of a periodic real field to n samples."""
+    c = np.fft.rfft(f)
+    c2 = np.zeros(n // 2 + 1, dtype=complex)
+    c2[: c.size - 1] = c[:-1]  # the old Nyquist term is dropped (a single cosine, ambiguous when padded)
+    return np.fft.irfft(c2, n) * (n / f.size)
+
+
+@pytest.mark.parametrize("ntau", [256, 1024, 2048])
+def test_boundary_kernels_shapes_vs_oracle(engine, oracle, ntau):
+    """Pack, unpack and both Taylor expansions at more samples than the C1
+    fixture has: the C1 fields interpolated spectrally to ntau points."""
+    d = load_case("c1_fixture")
+    cfg = d["cfg"]
+    up, psic, fc = (_interp_field(d[k], ntau) for k in ("unpack_up", "unpack_psic", "unpack_fc"))
+    z = engine.pack(ntau, up, psic, fc)
+    assert rel_err(z, oracle.pack(ntau, up, psic, fc)) < 1e-12
+    up2, psic2, fc2 = engine.unpack(ntau, z)
+    uo, po, fo = oracle.unpack(ntau, z)
+    for a, b in ((up2, uo), (psic2, po), (fc2, fo)):
+        assert rel_err(a, b) < 1e-12
+    delta = float(d["in0"][2 * d["in0"].size // 3 + 2])
+    yl, yr = engine.expansions(ntau, cfg["Dim"], delta, cfg["XLeft"], cfg["XRight"], fc, psic, up)
+    assert rel_err(yl, oracle.left_expansion(ntau, cfg["Dim"], cfg["XLeft"], fc, psic, delta)) < 1e-12
+    assert rel_err(yr, oracle.right_expansion(ntau, cfg["Dim"], cfg["XRight"], up, delta)) < 1e-12
+
+
 def test_grid_parity(engine):
     d = load_case("c3_fixture")
     s = _solve(engine, d["cfg"])
