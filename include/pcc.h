@@ -35,12 +35,13 @@ typedef enum {
     PCC_ERR_OOM = 3,
     PCC_ERR_IRK_NO_CONVERGENCE = 4, /* ShootingSolver.cpp:69-82,112-125 exit */
     PCC_ERR_DELTA_MISMATCH = 5,     /* ShootingSolver.cpp:167-178 exit */
-    PCC_ERR_NAN = 6,
+    PCC_ERR_NAN = 6,                /* non-finite free data given to a host-pointer entry point */
     PCC_ERR_LU_SINGULAR = 7,        /* NewtonSolver.cpp:751-755 exit */
     PCC_ERR_IR_STALL = 8,
     PCC_ERR_UNSUPPORTED = 9,
     PCC_ERR_NEWTON_NO_CONVERGENCE = 10, /* NewtonSolver.cpp:368-372 exit */
-    PCC_ERR_BUSY = 11
+    PCC_ERR_BUSY = 11,
+    PCC_ERR_TIMEOUT = 12            /* pcc_wait: the solve had not ended by the deadline */
 } pcc_status;
 
 typedef enum {
@@ -256,7 +257,8 @@ pcc_status pcc_submit(pcc_ctx* ctx, const pcc_request* req, uint64_t* ticket);
 /* Non-blocking: out->done tells whether the solve has ended; x_out (optional,
  * Nnewton) receives the result iterate once it has. */
 pcc_status pcc_poll(pcc_ctx* ctx, uint64_t ticket, pcc_result* out, double* x_out);
-/* As pcc_poll, waiting up to timeout_s seconds for the solve to end. */
+/* As pcc_poll, waiting up to timeout_s seconds for the solve to end;
+ * PCC_ERR_TIMEOUT (out filled, out->done = 0) if it has not ended by then. */
 pcc_status pcc_wait(pcc_ctx* ctx, uint64_t ticket, double timeout_s, pcc_result* out, double* x_out);
 pcc_status pcc_serve_stats(pcc_ctx* ctx, pcc_serve_info* out);
 /* Finishes every submitted request, then stops the loop and drops the results. */

@@ -41,7 +41,8 @@ const char* kStatusNames[] = {"PCC_OK",
                               "PCC_ERR_IR_STALL",
                               "PCC_ERR_UNSUPPORTED",
                               "PCC_ERR_NEWTON_NO_CONVERGENCE",
-                              "PCC_ERR_BUSY"};
+                              "PCC_ERR_BUSY",
+                              "PCC_ERR_TIMEOUT"};
 
 // Gauss-Legendre tableaux exactly as ODEStepper.cpp:27-79 builds them.
 int tableau(int scheme, double a[3][3], double b[3], double c[3])
@@ -845,6 +846,7 @@ pcc_status pcc_jacobian_columns(pcc_solve* s, const double* in0, const double* o
 pcc_status pcc_shoot(pcc_solve* s, const double* in0, double* out0, pcc_stats* stats)
 {
     if (!s || !in0 || !out0) return PCC_ERR_INVALID_ARG;
+    if (!all_finite(in0, s->nn)) return fail(s->ctx, PCC_ERR_NAN, "non-finite value in the free data");
     return pcc_jacobian_columns(s, in0, nullptr, s->nn, s->nn + 1, out0, stats);
 }
 
@@ -852,6 +854,7 @@ pcc_status pcc_shoot_debug(pcc_solve* s, const double* in0, double* out0, int de
                            int* grid_idx, double* fields, pcc_stats* stats)
 {
     if (!s || !in0 || !out0 || !count || debug_nx < 1 || max_snaps < 0) return PCC_ERR_INVALID_ARG;
+    if (!all_finite(in0, s->nn)) return fail(s->ctx, PCC_ERR_NAN, "non-finite value in the free data");
     pcc_ctx* ctx = s->ctx;
     const int nl = s->d.nl, nr = s->d.nr, n = s->d.ntau, nn = s->nn;
     // snapshot grid indices in the reference's export order
@@ -994,6 +997,7 @@ pcc_status pcc_solve_sync(pcc_solve* s, pcc_stats* stats)
 pcc_status pcc_jacobian(pcc_solve* s, const double* in0, const double* out0, double* J, pcc_stats* stats)
 {
     if (!s || !in0 || !out0 || !J) return PCC_ERR_INVALID_ARG;
+    if (!all_finite(in0, s->nn) || !all_finite(out0, s->nn)) return fail(s->ctx, PCC_ERR_NAN, "non-finite value in the free data");
     pcc_ctx* ctx = s->ctx;
     PCC_CUDA(ctx, cudaSetDevice(ctx->device));
     const int nn = s->nn;
@@ -1008,6 +1012,7 @@ pcc_status pcc_jacobian(pcc_solve* s, const double* in0, const double* out0, dou
 pcc_status pcc_boundary_data(pcc_solve* s, const double* in0, double* y_left, double* y_right)
 {
     if (!s || !in0 || !y_left || !y_right) return PCC_ERR_INVALID_ARG;
+    if (!all_finite(in0, s->nn)) return fail(s->ctx, PCC_ERR_NAN, "non-finite value in the free data");
     pcc_ctx* ctx = s->ctx;
     PCC_CUDA(ctx, cudaSetDevice(ctx->device));
     const int nn = s->nn, n = s->d.ntau;
@@ -1240,6 +1245,7 @@ pcc_status pcc_newton_step(pcc_solve* s, double* in0, double* err_out, pcc_preci
                            pcc_refine_report* report)
 {
     if (!s || !in0) return PCC_ERR_INVALID_ARG;
+    if (!all_finite(in0, s->nn)) return fail(s->ctx, PCC_ERR_NAN, "non-finite value in the free data");
     pcc_ctx* ctx = s->ctx;
     PCC_CUDA(ctx, cudaSetDevice(ctx->device));
     const int nn = s->nn;
@@ -1454,6 +1460,7 @@ pcc_status pcc_jacobian_batch(pcc_ctx* ctx, int count, pcc_solve* const* solves,
     std::vector<pcc_solve*> v(solves, solves + count);
     for (int i = 0; i < count; ++i) {
         if (!v[i] || v[i]->ctx != ctx || !in0[i] || !out0[i] || !J[i]) return PCC_ERR_INVALID_ARG;
+        if (!all_finite(in0[i], v[i]->nn) || !all_finite(out0[i], v[i]->nn)) return fail(ctx, PCC_ERR_NAN, "non-finite value in the free data");
         if (!march_batch_supported(v[i]->d.ntau, v[i]->stages))
             return fail(ctx, PCC_ERR_UNSUPPORTED, "batch: Ntau must be 128..1024 with 2 IRK stages");
         for (int j = 0; j < i; ++j)
@@ -1502,6 +1509,7 @@ pcc_status pcc_jacobian_batch(pcc_ctx* ctx, int count, pcc_solve* const* solves,
 pcc_status pcc_newton_begin(pcc_solve* s, const double* in0)
 {
     if (!s || !in0) return PCC_ERR_INVALID_ARG;
+    if (!all_finite(in0, s->nn)) return fail(s->ctx, PCC_ERR_NAN, "non-finite value in the free data");
     pcc_ctx* ctx = s->ctx;
     PCC_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;

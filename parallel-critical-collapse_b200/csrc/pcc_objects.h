@@ -1,6 +1,7 @@
 // pcc_objects.h -- the opaque objects of include/pcc.h and the error helpers
 // shared by the translation units that implement the C ABI.
 #pragma once
+#include <cmath>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -123,6 +124,15 @@ inline pcc_status fail(pcc_ctx* ctx, pcc_status s, const std::string& msg)
         ctx->last_error = msg;
     }
     return s;
+}
+
+// Free data handed in through host pointers must be finite: a NaN or an
+// infinity would only surface later as a failed IRK iteration.
+inline bool all_finite(const double* v, int n)
+{
+    for (int i = 0; i < n; ++i)
+        if (!std::isfinite(v[i])) return false;
+    return true;
 }
 
 }  // namespace pcc

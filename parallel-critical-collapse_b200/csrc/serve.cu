@@ -487,6 +487,8 @@ pcc_status pcc_submit(pcc_ctx* ctx, const pcc_request* req, uint64_t* ticket)
         return fail(ctx, PCC_ERR_INVALID_ARG, "Ntau must be 128..2048, power of two");
     if (!march_batch_supported(req->desc.ntau, req->desc.scheme))
         return fail(ctx, PCC_ERR_UNSUPPORTED, "serving batches Ntau 128..1024 with 2 IRK stages");
+    if (!all_finite(req->in0, 3 * req->desc.ntau / 4))
+        return fail(ctx, PCC_ERR_NAN, "non-finite value in the free data");
     if (!ctx->server) {
         pcc_status r = pcc_serve_start(ctx, nullptr);
         if (r != PCC_OK) return r;
@@ -544,9 +546,9 @@ pcc_status pcc_wait(pcc_ctx* ctx, uint64_t ticket, double timeout_s, pcc_result*
     if (it == sv->records.end()) return PCC_ERR_INVALID_ARG;
     const auto until = Clock::now() + std::chrono::duration_cast<Clock::duration>(
                                           std::chrono::duration<double>(timeout_s < 0 ? 0.0 : timeout_s));
-    sv->cv_done.wait_until(lk, until, [&] { return sv->records[ticket].done; });
+    const bool done = sv->cv_done.wait_until(lk, until, [&] { return sv->records[ticket].done; });
     fill_result(sv->records[ticket], out, x_out);
-    return PCC_OK;
+    return done ? PCC_OK : PCC_ERR_TIMEOUT;
 }
 
 pcc_status pcc_serve_stats(pcc_ctx* ctx, pcc_serve_info* out)

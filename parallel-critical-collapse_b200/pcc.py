@@ -26,8 +26,9 @@ _I = ctypes.POINTER(ctypes.c_int)
 
 STATUS = ["PCC_OK", "PCC_ERR_INVALID_ARG", "PCC_ERR_CUDA", "PCC_ERR_OOM", "PCC_ERR_IRK_NO_CONVERGENCE",
           "PCC_ERR_DELTA_MISMATCH", "PCC_ERR_NAN", "PCC_ERR_LU_SINGULAR", "PCC_ERR_IR_STALL", "PCC_ERR_UNSUPPORTED",
-          "PCC_ERR_NEWTON_NO_CONVERGENCE", "PCC_ERR_BUSY"]
+          "PCC_ERR_NEWTON_NO_CONVERGENCE", "PCC_ERR_BUSY", "PCC_ERR_TIMEOUT"]
 PREC_FP64, PREC_MIXED = 0, 1
+PCC_ERR_NAN, PCC_ERR_TIMEOUT = 6, 12
 
 # every function include/pcc.h declares
 EXPORTS = ["pcc_ctx_create", "pcc_ctx_destroy", "pcc_status_string", "pcc_last_error", "pcc_solve_create",
@@ -361,7 +362,9 @@ class Engine:
     def _result(self, fn, ticket, *args):
         r = Result()
         x = np.zeros(self._ticket_nn[ticket])
-        self._check(fn(self.ctx, ctypes.c_uint64(ticket), *args, ctypes.byref(r), _p(x)))
+        st = fn(self.ctx, ctypes.c_uint64(ticket), *args, ctypes.byref(r), _p(x))
+        if st != PCC_ERR_TIMEOUT:
+            self._check(st)
         d = r.as_dict()
         return d, (x if r.done else None)
 
@@ -370,6 +373,7 @@ class Engine:
         return self._result(self.lib.pcc_poll, ticket)
 
     def wait(self, ticket, timeout_s=600.0):
+        """As poll, blocking up to timeout_s; on timeout x is None and done is 0."""
         return self._result(self.lib.pcc_wait, ticket, ctypes.c_double(timeout_s))
 
     def serve_stats(self):

@@ -308,6 +308,26 @@ def test_irk_no_convergence_is_reported(engine):
     assert np.max(np.abs(out0 - d["out0"])) < 1e-10
 
 
+def test_non_finite_free_data_is_refused(engine):
+    """A NaN or an infinity in the free data handed in through host pointers
+    is refused with PCC_ERR_NAN before any launch (the reference would run
+    into an IRK failure and exit); the context stays usable."""
+    import pcc
+
+    d = load_case("c1_fixture")
+    s = _solve(engine, d["cfg"])
+    bad = d["in0"].copy()
+    bad[7] = np.nan
+    for call in (lambda: s.shoot(bad), lambda: s.jacobian(bad, d["out0"]),
+                 lambda: s.jacobian(d["in0"], np.where(np.arange(bad.size) == 3, np.inf, d["out0"])),
+                 lambda: engine.newton_solve([s], [bad])):
+        with pytest.raises(pcc.PccError) as e:
+            call()
+        assert e.value.status == pcc.PCC_ERR_NAN
+    out0 = s.shoot(d["in0"])
+    assert np.max(np.abs(out0 - d["out0"])) < 1e-10
+
+
 def test_invalid_arguments(engine):
     import pcc
 

@@ -108,3 +108,31 @@ def test_serve_reports_irk_failure(engine):
         assert np.array_equal(x, c1["in0"])
     finally:
         engine.serve_stop()
+
+
+def test_serve_wait_times_out_and_rejects_non_finite_input(engine):
+    """pcc_wait returns PCC_ERR_TIMEOUT (result not done) when the solve has
+    not ended by its deadline, and the solve still completes; a request whose
+    free data hold a NaN is refused at submission with PCC_ERR_NAN."""
+    import ctypes
+
+    import pcc
+
+    c1 = load_case("c1_newton")
+    engine.serve_start()
+    try:
+        t = engine.submit(_cfg(c1, PrecisionNewton=1e-12, MaxIterNewton=12), c1["in0"])
+        r = pcc.Result()
+        x = np.zeros(c1["in0"].size)
+        st = engine.lib.pcc_wait(engine.ctx, ctypes.c_uint64(t), ctypes.c_double(0.0), ctypes.byref(r),
+                                 x.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        assert st == pcc.PCC_ERR_TIMEOUT and r.done == 0
+        res, xs = engine.wait(t)
+        assert res["done"] == 1 and res["status"] == 0 and xs is not None
+        bad = c1["in0"].copy()
+        bad[5] = np.nan
+        with pytest.raises(pcc.PccError) as e:
+            engine.submit(_cfg(c1), bad)
+        assert e.value.status == pcc.PCC_ERR_NAN
+    finally:
+        engine.serve_stop()
