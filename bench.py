@@ -50,6 +50,21 @@ def workload(seed, amp):
     return cfg, perturb(d["in0"], np.random.default_rng(seed), amp)
 
 
+# Seeds of the C3 free data whose base shoot converges (checked on a B200 over
+# seeds 1024..1199: at perturbation amplitude 0.1 most seeds march into an IRK
+# failure).  Rank r of a multi-GPU run with the default seed takes the r-th,
+# so that every GPU builds the Jacobian of a solve of its own.
+C3_SEEDS = (1024, 1031, 1034, 1046, 1058, 1075, 1090, 1091, 1100, 1117, 1122, 1124, 1128, 1156, 1163, 1178)
+
+
+def rank_seed(seed, rank):
+    """The free-data seed of a rank: the validated list for the default seed,
+    else seed + rank."""
+    if seed == C3_SEEDS[0]:
+        return C3_SEEDS[rank % len(C3_SEEDS)]
+    return seed + rank
+
+
 def perturb(z, rng, amp):
     """The free-data perturbation of workload(): per field, amp * |c_lead| *
     N(0,1) * exp(-k/8) on the coefficient of mode k (Delta and the shared
@@ -488,7 +503,7 @@ def run_engine(args, world, rank, local):
 
     torch.cuda.set_device(local)
     eng = pcc.Engine(local)
-    cfg, in0 = workload(args.seed + rank, args.amp)
+    cfg, in0 = workload(rank_seed(args.seed, rank), args.amp)
     solve = eng.solve(pcc.SolveDesc.from_config(cfg))
     nn, n = solve.nn, solve.ntau
     out0 = solve.shoot(in0)  # base shoot (the Newton step's, outside the build)
@@ -589,6 +604,7 @@ def run_engine(args, world, rank, local):
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded free data)",
                 "config": {"workload": "C3: D=4, Ntau=1024, 4000+4000 points, 768-column FD Jacobian, IRK2",
                            "ntau": n, "points": cfg["NLeft"] + cfg["NRight"], "columns": nn, "seed": args.seed,
+                           "rank_seeds": [rank_seed(args.seed, r) for r in range(world)],
                            "amp": args.amp, "l2": "flushed (256 MB write) before every timed build",
                            "parallelism": f"{world} independent solves, one per GPU",
                            "sweep_ctas": st_e.sweep_ctas, "wall_s": wall,
