@@ -583,11 +583,13 @@ def run_engine(args, world, rank, local):
                 "flops_per_launch": flops_per_launch, "rhs_evals_per_launch": rhs / args.steps,
                 "flop_convention": "7*5*N*log2(N) + 100*N per RHS evaluation (reference algorithm)"}
 
-    predictor = predictor_build(eng, cfg, in0, out0, h_J.numpy().copy(), args.steps, flush) \
-        if not args.quick else None
-    newton = newton_compare(eng, cfg, in0, out0, h_J.numpy().copy()) if not args.quick else None
-    dscan = run_dscan(eng, args) if not args.quick else None
-    serving = run_serving(eng, args, args.rate, args.requests) if not args.quick else None
+    # the further sections go into rank 0's line only, so only rank 0 runs
+    # them (after the last collective): another rank's seed need not suit them
+    extras = rank == 0 and not args.quick
+    predictor = predictor_build(eng, cfg, in0, out0, h_J.numpy().copy(), args.steps, flush) if extras else None
+    newton = newton_compare(eng, cfg, in0, out0, h_J.numpy().copy()) if extras else None
+    dscan = run_dscan(eng, args) if extras else None
+    serving = run_serving(eng, args, args.rate, args.requests) if extras else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
