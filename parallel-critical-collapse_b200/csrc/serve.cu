@@ -343,26 +343,39 @@ bool Server::start_launches()
         for (auto& a : active)
             if (a->phase == 1 && a->next_item < a->n_items) ready.push_back(a.get());
         if (ready.empty()) break;
-        // about one wave: round-robin over the solves, one CTA's worth of sweeps per turn
+        // About one wave of sweeps, shortest work first: the solve admitted
+        // longest ago gets one CTA's worth first (no solve waits for ever),
+        // then the wave fills with the solves whose Newton iteration is the
+        // least work (sweeps x steps x Ntau log2 Ntau), each taking all of
+        // its remaining sweeps, so that small solves finish early instead of
+        // sharing every wave with large ones.  Throughput is the same; a
+        // solve's results do not depend on the mix.
         const int capacity = 2 * ctx->sms;
+        auto work = [](const Active* a) {
+            const double n = a->s->d.ntau;
+            return (double)a->n_items * (a->s->d.nl + a->s->d.nr) * n * std::log2(n);
+        };
+        std::stable_sort(ready.begin(), ready.end(),
+                         [&](const Active* x, const Active* y) { return work(x) < work(y); });
+        size_t oldest = 0;
+        for (size_t i = 1; i < ready.size(); ++i)
+            if (ready[i]->t_admit < ready[oldest]->t_admit) oldest = i;
         std::vector<BatchItem> items;
         std::vector<int> taken(ready.size(), 0);
         double ctas = 0.0;
-        bool any = true;
-        while (ctas < capacity && any) {
-            any = false;
-            for (size_t i = 0; i < ready.size() && ctas < capacity; ++i) {
-                Active& a = *ready[i];
-                const int spc = sweeps_per_cta(a.s->d.ntau);
-                const int take = std::min(spc, a.n_items - a.next_item);
-                if (take <= 0) continue;
-                for (int j = 0; j < take; ++j) items.push_back({a.s, a.next_item + j});
-                a.next_item += take;
-                taken[i] += take;
-                ctas += (double)take / spc;
-                any = true;
-            }
-        }
+        auto give = [&](size_t i, int limit) {
+            Active& a = *ready[i];
+            const int spc = sweeps_per_cta(a.s->d.ntau);
+            const int take = std::min({limit, a.n_items - a.next_item,
+                                       (int)std::ceil((capacity - ctas) * spc)});
+            if (take <= 0) return;
+            for (int j = 0; j < take; ++j) items.push_back({a.s, a.next_item + j});
+            a.next_item += take;
+            taken[i] += take;
+            ctas += (double)take / spc;
+        };
+        give(oldest, sweeps_per_cta(ready[oldest]->s->d.ntau));
+        for (size_t i = 0; i < ready.size() && ctas < capacity; ++i) give(i, ready[i]->n_items);
         L.parts.clear();
         for (size_t i = 0; i < ready.size(); ++i)
             if (taken[i]) {
