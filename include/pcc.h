@@ -220,7 +220,8 @@ pcc_status pcc_newton_solve(pcc_ctx* ctx, int count, pcc_solve* const* solves, d
  * concurrent solves), keeps each solve's Newton state on the device, and
  * batches the sweeps of all admitted solves as they become ready into shared
  * persistent launches, so that requests arriving while others run overlap
- * with them on the device.  Each result equals the one the same request gives
+ * with them on the device.  Each launch is filled shortest work first (the
+ * longest-waiting solve always gets a share), so small solves finish early.  Each result equals the one the same request gives
  * alone.  Ntau 128..1024 with 2 IRK stages.  While serving runs, the context
  * takes only pcc_submit / pcc_poll / pcc_wait / pcc_serve_stats, from any
  * thread; results can be read until pcc_serve_stop. */
