@@ -256,13 +256,23 @@ pcc_status pcc_serve_start(pcc_ctx* ctx, const pcc_serve_opts* opts);
 /* Queues a request; ticket identifies it in pcc_poll / pcc_wait. */
 pcc_status pcc_submit(pcc_ctx* ctx, const pcc_request* req, uint64_t* ticket);
 /* Non-blocking: out->done tells whether the solve has ended; x_out (optional,
- * Nnewton) receives the result iterate once it has. */
+ * Nnewton) receives the result iterate once it has.  A finished result is
+ * handed out once: the pcc_poll or pcc_wait call that returns it with
+ * done = 1 releases its record, and later calls with that ticket return
+ * PCC_ERR_INVALID_ARG (so a long-running service holds no memory for results
+ * it has delivered). */
 pcc_status pcc_poll(pcc_ctx* ctx, uint64_t ticket, pcc_result* out, double* x_out);
 /* As pcc_poll, waiting up to timeout_s seconds for the solve to end;
- * PCC_ERR_TIMEOUT (out filled, out->done = 0) if it has not ended by then. */
+ * PCC_ERR_TIMEOUT (out filled, out->done = 0) if it has not ended by then,
+ * PCC_ERR_BUSY if serving was shut down (context destroyed) meanwhile. */
 pcc_status pcc_wait(pcc_ctx* ctx, uint64_t ticket, double timeout_s, pcc_result* out, double* x_out);
 pcc_status pcc_serve_stats(pcc_ctx* ctx, pcc_serve_info* out);
-/* Finishes every submitted request, then stops the loop and drops the results. */
+/* Finishes every submitted request (callers blocked in pcc_wait receive their
+ * results meanwhile), then stops the loop and drops the undelivered results.
+ * It may overlap pcc_poll / pcc_wait / pcc_submit on other threads: those
+ * return PCC_ERR_INVALID_ARG or PCC_ERR_BUSY once the loop has stopped, and
+ * the server is freed only after the last of them has returned.  A second
+ * concurrent pcc_serve_stop returns at once. */
 pcc_status pcc_serve_stop(pcc_ctx* ctx);
 
 /* ---- lower-level entry points (the reference's inner class methods) ---- */
@@ -305,9 +315,11 @@ pcc_status pcc_expansions(pcc_ctx* ctx, int ntau, double dim, double delta, doub
  * into the library (1.3 MiB, kept by every GPU that loads the library until
  * the process exits), so Ntau is limited to 2048; larger values are rejected
  * with PCC_ERR_INVALID_ARG.  The call is asynchronous on the context stream
- * and allocates nothing.  Its first call on a device looks up the array's
- * device address; make that first call before any stream capture.  All calls
- * share the one array, so calls that overlap on the GPU race. */
+ * and allocates nothing.  It makes the context's device current for its
+ * duration and restores the calling thread's current device before it
+ * returns.  Its first call on a device looks up the array's device address;
+ * make that first call before any stream capture.  All calls share the one
+ * array, so calls that overlap on the GPU race. */
 pcc_status pcc_expansions_static(pcc_ctx* ctx, int ntau, double dim, double delta, double x_l, double x_r,
                                  const double* d_fc, const double* d_psic, const double* d_up, double* d_y_left,
                                  double* d_y_right);

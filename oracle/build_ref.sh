@@ -22,6 +22,7 @@
 set -euo pipefail
 
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+# The reference checkout: $PCC_REFERENCE_ROOT, else /root/reference.
 REF="${PCC_REFERENCE_ROOT:-/root/reference}"
 OUT="$HERE/_ref"
 SITE="$(python3 -c 'import sysconfig; print(sysconfig.get_paths()["purelib"])')"

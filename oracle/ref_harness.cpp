@@ -216,7 +216,7 @@ int ref_jacobian_columns(const char* cfg_json, const double* in0, const double* 
         vec_complex yl(ntau), yr(ntau), mm(ntau);
         InitialConditionGenerator g(ntau, cfg.Dim, cfg.Delta);
         ShootingSolver sh((int)ntau, cfg.Dim, cfg.PrecisionIRK, g, cfg.MaxIterIRK, cfg.SchemeIRK);
-#pragma omp for schedule(dynamic, 1)
+#pragma omp for schedule(static)
         for (int c = c0; c < c1; ++c) {
             vec_real pin = base_in;
             pin[c] += cfg.EpsNewton;

@@ -113,8 +113,9 @@ def build_oracle(force=False):
     import oracle_lib  # noqa: E402  (test infrastructure: the checker, built beside the product)
 
     oracle_lib.build(force=force)
-    ref = Path(os.environ.get("PCC_REFERENCE_ROOT", "/root/reference"))
-    if (ref / "src").is_dir() and (force or not (REPO / "oracle" / "_ref" / "libpcc_ref.so").exists()):
+    # the compiled reference: oracle/build_ref.sh finds the reference checkout
+    # itself and keeps the prebuilt oracle/_ref where there is none
+    if force or not (REPO / "oracle" / "_ref" / "libpcc_ref.so").exists():
         subprocess.run(["bash", str(REPO / "oracle" / "build_ref.sh")], check=True)
 
 

@@ -36,7 +36,8 @@ struct pcc_ctx {
     void* lu_work = nullptr;
     size_t lu_work_bytes = 0;
     pcc::BatchTables batch;         // tables of the synchronous batch entry points
-    pcc::Server* server = nullptr;  // serving loop (serve.cu)
+    pcc::Server* server = nullptr;  // serving loop (serve.cu), guarded by serve_mu
+    std::mutex serve_mu;            // start, stop and the lookups of pcc_submit/poll/wait/stats
 };
 
 struct pcc_solve {

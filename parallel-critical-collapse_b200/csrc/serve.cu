@@ -16,10 +16,22 @@
 //              state tells the loop whether to start the next iteration;
 //   sweeps     the sweeps of every solve whose boundary data are ready are
 //              pooled, and batch march launches of about one wave each take
-//              them round-robin over the solves (one CTA's worth per turn);
-//              two launches are in flight on low-priority streams, so a launch
-//              that drains leaves its SMs to the next one, and to the
+//              them shortest work first (the solve admitted longest ago gets
+//              one CTA's worth, then the solves with the least work per Newton
+//              iteration take all their remaining sweeps until the wave is
+//              full); two launches are in flight on low-priority streams, so a
+//              launch that drains leaves its SMs to the next one, and to the
 //              high-priority per-solve kernels first.
+//
+// Threads.  pcc_submit / pcc_poll / pcc_wait / pcc_serve_stats may be called
+// from any thread while serving runs.  Each holds the server as a "user" for
+// its duration (ctx->serve_mu guards the pointer, Server::users counts the
+// holders); pcc_serve_stop first lets the loop finish every submitted request,
+// then unpublishes the server, wakes the waiters still blocked in pcc_wait
+// (they return PCC_ERR_BUSY) and deletes it only once no user is left.  A
+// finished result is handed out once: the pcc_poll or pcc_wait call that
+// returns it with done = 1 erases the record, so a long-running service keeps
+// no per-request memory for results already delivered.
 //
 // Newton state stays on the device for the whole solve; the host reads one
 // small record per iteration.  A solve's result does not depend on the mix it
@@ -104,6 +116,9 @@ struct Server {
     std::map<uint64_t, ServeRecord> records;
     uint64_t next_ticket = 1;
     std::atomic<bool> stop{false}, abort{false};
+    int users = 0;          // API calls holding the server (pcc_submit/poll/wait/stats)
+    bool closing = false;   // pcc_serve_stop has unpublished the server
+    bool stop_claimed = false;  // a pcc_serve_stop call owns the shutdown (guarded by ctx->serve_mu)
     std::string fatal;
     long long submitted = 0, completed = 0, launches_done = 0, sweeps_done = 0;
     int n_active = 0, n_waiting = 0;
@@ -442,7 +457,12 @@ void Server::loop()
 
 void server_shutdown(pcc_ctx* ctx)
 {
-    Server* sv = ctx ? ctx->server : nullptr;
+    Server* sv = nullptr;
+    if (ctx) {
+        std::lock_guard<std::mutex> g(ctx->serve_mu);
+        sv = ctx->server;
+        ctx->server = nullptr;  // no new user can take it from here on
+    }
     if (!sv) return;
     {
         std::lock_guard<std::mutex> lk(sv->mu);
@@ -451,12 +471,19 @@ void server_shutdown(pcc_ctx* ctx)
     }
     sv->cv_submit.notify_all();
     if (sv->th.joinable()) sv->th.join();
+    {
+        // wake the callers still blocked in pcc_wait (they return
+        // PCC_ERR_BUSY) and wait until every user has left
+        std::unique_lock<std::mutex> lk(sv->mu);
+        sv->closing = true;
+        sv->cv_done.notify_all();
+        sv->cv_done.wait(lk, [&] { return sv->users == 0; });
+    }
     for (Launch& L : sv->launches) {
         batch_tables_free(L.tab);
         if (L.st) cudaStreamDestroy(L.st);
     }
     if (sv->h_slots) cudaFreeHost(sv->h_slots);
-    ctx->server = nullptr;
     delete sv;
 }
 
@@ -464,12 +491,12 @@ void server_shutdown(pcc_ctx* ctx)
 
 using namespace pcc;
 
-extern "C" {
+namespace {
 
-pcc_status pcc_serve_start(pcc_ctx* ctx, const pcc_serve_opts* opts)
+// Starts the loop; the caller holds ctx->serve_mu and has checked that no
+// server runs.
+pcc_status serve_start_locked(pcc_ctx* ctx, const pcc_serve_opts* opts)
 {
-    if (!ctx) return PCC_ERR_INVALID_ARG;
-    if (ctx->server) return fail(ctx, PCC_ERR_BUSY, "serving already started");
     if (opts && opts->max_active < 0) return PCC_ERR_INVALID_ARG;
     PCC_CUDA(ctx, cudaSetDevice(ctx->device));
     auto sv = std::make_unique<Server>();
@@ -492,6 +519,45 @@ pcc_status pcc_serve_start(pcc_ctx* ctx, const pcc_serve_opts* opts)
     return PCC_OK;
 }
 
+// The running server, held as a user until release(); null when none runs or
+// it is being stopped.
+Server* acquire(pcc_ctx* ctx)
+{
+    std::lock_guard<std::mutex> g(ctx->serve_mu);
+    Server* sv = ctx->server;
+    if (!sv) return nullptr;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->users += 1;
+    return sv;
+}
+
+void release(Server* sv)
+{
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->users -= 1;
+    if (sv->closing) sv->cv_done.notify_all();
+}
+
+struct UserGuard {
+    Server* sv;
+    ~UserGuard()
+    {
+        if (sv) release(sv);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+pcc_status pcc_serve_start(pcc_ctx* ctx, const pcc_serve_opts* opts)
+{
+    if (!ctx) return PCC_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> g(ctx->serve_mu);
+    if (ctx->server) return fail(ctx, PCC_ERR_BUSY, "serving already started");
+    return serve_start_locked(ctx, opts);
+}
+
 pcc_status pcc_submit(pcc_ctx* ctx, const pcc_request* req, uint64_t* ticket)
 {
     if (!ctx || !req || !req->in0 || !ticket) return PCC_ERR_INVALID_ARG;
@@ -502,11 +568,17 @@ pcc_status pcc_submit(pcc_ctx* ctx, const pcc_request* req, uint64_t* ticket)
         return fail(ctx, PCC_ERR_UNSUPPORTED, "serving batches Ntau 128..1024 with 2 IRK stages");
     if (!all_finite(req->in0, 3 * req->desc.ntau / 4))
         return fail(ctx, PCC_ERR_NAN, "non-finite value in the free data");
-    if (!ctx->server) {
-        pcc_status r = pcc_serve_start(ctx, nullptr);
-        if (r != PCC_OK) return r;
+    {
+        // the lazy start: two first submits from different threads start one loop
+        std::lock_guard<std::mutex> g(ctx->serve_mu);
+        if (!ctx->server) {
+            pcc_status r = serve_start_locked(ctx, nullptr);
+            if (r != PCC_OK) return r;
+        }
     }
-    Server* sv = ctx->server;
+    Server* sv = acquire(ctx);
+    if (!sv) return fail(ctx, PCC_ERR_BUSY, "serving is stopping");
+    UserGuard hold{sv};
     ServeRequest r;
     r.desc = req->desc;
     r.in0.assign(req->in0, req->in0 + 3 * req->desc.ntau / 4);
@@ -541,35 +613,52 @@ static void fill_result(const ServeRecord& rec, pcc_result* out, double* x_out)
 
 pcc_status pcc_poll(pcc_ctx* ctx, uint64_t ticket, pcc_result* out, double* x_out)
 {
-    if (!ctx || !ctx->server) return PCC_ERR_INVALID_ARG;
-    Server* sv = ctx->server;
+    if (!ctx) return PCC_ERR_INVALID_ARG;
+    Server* sv = acquire(ctx);
+    if (!sv) return PCC_ERR_INVALID_ARG;
+    UserGuard hold{sv};
     std::lock_guard<std::mutex> lk(sv->mu);
     auto it = sv->records.find(ticket);
     if (it == sv->records.end()) return PCC_ERR_INVALID_ARG;
     fill_result(it->second, out, x_out);
+    if (it->second.done) sv->records.erase(it);  // delivered: a result is handed out once
     return PCC_OK;
 }
 
 pcc_status pcc_wait(pcc_ctx* ctx, uint64_t ticket, double timeout_s, pcc_result* out, double* x_out)
 {
-    if (!ctx || !ctx->server) return PCC_ERR_INVALID_ARG;
-    Server* sv = ctx->server;
+    if (!ctx) return PCC_ERR_INVALID_ARG;
+    Server* sv = acquire(ctx);
+    if (!sv) return PCC_ERR_INVALID_ARG;
+    UserGuard hold{sv};
     std::unique_lock<std::mutex> lk(sv->mu);
-    auto it = sv->records.find(ticket);
-    if (it == sv->records.end()) return PCC_ERR_INVALID_ARG;
+    if (sv->records.find(ticket) == sv->records.end()) return PCC_ERR_INVALID_ARG;
     const auto until = Clock::now() + std::chrono::duration_cast<Clock::duration>(
                                           std::chrono::duration<double>(timeout_s < 0 ? 0.0 : timeout_s));
-    const bool done = sv->cv_done.wait_until(lk, until, [&] { return sv->records[ticket].done; });
-    fill_result(sv->records[ticket], out, x_out);
-    return done ? PCC_OK : PCC_ERR_TIMEOUT;
+    // records are erased only by the call that delivers them, so the ticket's
+    // record stays while this call waits (unless another thread takes it)
+    auto ready = [&] {
+        auto it = sv->records.find(ticket);
+        return it == sv->records.end() || it->second.done || sv->closing;
+    };
+    sv->cv_done.wait_until(lk, until, ready);
+    auto it = sv->records.find(ticket);
+    if (it == sv->records.end()) return PCC_ERR_INVALID_ARG;  // delivered to another caller meanwhile
+    fill_result(it->second, out, x_out);
+    if (it->second.done) {
+        sv->records.erase(it);
+        return PCC_OK;
+    }
+    return sv->closing ? PCC_ERR_BUSY : PCC_ERR_TIMEOUT;
 }
 
 pcc_status pcc_serve_stats(pcc_ctx* ctx, pcc_serve_info* out)
 {
     if (!ctx || !out) return PCC_ERR_INVALID_ARG;
     std::memset(out, 0, sizeof(*out));
-    Server* sv = ctx->server;
+    Server* sv = acquire(ctx);
     if (!sv) return PCC_OK;
+    UserGuard hold{sv};
     std::lock_guard<std::mutex> lk(sv->mu);
     out->submitted = sv->submitted;
     out->completed = sv->completed;
@@ -585,14 +674,19 @@ pcc_status pcc_serve_stats(pcc_ctx* ctx, pcc_serve_info* out)
 pcc_status pcc_serve_stop(pcc_ctx* ctx)
 {
     if (!ctx) return PCC_ERR_INVALID_ARG;
-    Server* sv = ctx->server;
-    if (!sv) return PCC_OK;
+    Server* sv = nullptr;
+    {
+        std::lock_guard<std::mutex> g(ctx->serve_mu);
+        sv = ctx->server;
+        if (!sv || sv->stop_claimed) return PCC_OK;  // not running, or another call is stopping it
+        sv->stop_claimed = true;
+    }
     {
         std::lock_guard<std::mutex> lk(sv->mu);
         sv->stop = true;  // finish everything submitted, then leave
     }
     sv->cv_submit.notify_all();
-    if (sv->th.joinable()) sv->th.join();
+    if (sv->th.joinable()) sv->th.join();  // waiters keep receiving results meanwhile
     std::string fatal = sv->fatal;
     server_shutdown(ctx);
     if (!fatal.empty()) return fail(ctx, PCC_ERR_CUDA, "serving loop: " + fatal);

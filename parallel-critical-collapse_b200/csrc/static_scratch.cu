@@ -34,7 +34,10 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 double* g_addr[kMaxDevices] = {};
 
-// exp(+2 pi i k/n) for k < n, written by the device into the static area
+// exp(+2 pi i k/n) for k < n, written by the device into the static area.
+// pcc_expansions takes the same table from the host (computed in long double
+// and rounded); sincospi's results differ from it by at most about one ulp,
+// which the 1e-12 parity check of the two entry points covers.
 __global__ void static_twiddle_kernel(double2* tw, int n)
 {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -65,7 +68,26 @@ extern "C" pcc_status pcc_expansions_static(pcc_ctx* ctx, int ntau, double dim, 
         return PCC_ERR_INVALID_ARG;
     }
     const int dev = pcc_ctx_device(ctx);
-    if (dev < 0 || dev >= kMaxDevices || cudaSetDevice(dev) != cudaSuccess) return PCC_ERR_CUDA;
+    if (dev < 0 || dev >= kMaxDevices) {
+        pcc_ctx_set_error(ctx, "pcc_expansions_static: device index out of range");
+        return PCC_ERR_INVALID_ARG;
+    }
+    // the context's device is made current for the call and the caller's
+    // current device is restored before returning
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    struct Restore {
+        int d;
+        ~Restore()
+        {
+            if (d >= 0) cudaSetDevice(d);
+        }
+    } restore{prev};
+    cudaError_t e = cudaSetDevice(dev);
+    if (e != cudaSuccess) {
+        pcc_ctx_set_error(ctx, cudaGetErrorString(e));
+        return PCC_ERR_CUDA;
+    }
     double* base = nullptr;
     {
         // set-up, once per device, with that device current: the device
@@ -73,7 +95,7 @@ extern "C" pcc_status pcc_expansions_static(pcc_ctx* ctx, int ntau, double dim, 
         std::lock_guard<std::mutex> lock(g_mu);
         if (!g_addr[dev]) {
             void* p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+            e = cudaGetSymbolAddress(&p, g_static_scratch);
             if (e != cudaSuccess || !p) {
                 pcc_ctx_set_error(ctx, cudaGetErrorString(e));
                 return PCC_ERR_CUDA;
@@ -85,9 +107,14 @@ extern "C" pcc_status pcc_expansions_static(pcc_ctx* ctx, int ntau, double dim, 
     cudaStream_t st = pcc_ctx_stream(ctx);
     double2* tw = reinterpret_cast<double2*>(base + kStaticWork);
     static_twiddle_kernel<<<(ntau + 255) / 256, 256, 0, st>>>(tw, ntau);
-    if (cudaGetLastError() != cudaSuccess) return PCC_ERR_CUDA;
-    // every work array is written before it is read, so nothing needs clearing
-    const cudaError_t e = launch_expansions(ntau, dim, delta, x_l, x_r, tw, base, d_fc, d_psic, d_up, d_y_left,
-                                            d_y_right, st);
-    return e == cudaSuccess ? PCC_OK : PCC_ERR_CUDA;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        // every work array is written before it is read, so nothing needs clearing
+        e = launch_expansions(ntau, dim, delta, x_l, x_r, tw, base, d_fc, d_psic, d_up, d_y_left, d_y_right, st);
+    }
+    if (e != cudaSuccess) {
+        pcc_ctx_set_error(ctx, cudaGetErrorString(e));
+        return PCC_ERR_CUDA;
+    }
+    return PCC_OK;
 }

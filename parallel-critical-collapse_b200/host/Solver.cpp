@@ -312,7 +312,7 @@ void ShootingSolver::shoot(vec_complex& YLeft, vec_complex& YRight, const vec_re
         d.xl = gridX[iLeft];
         d.xm = gridX[iMid];
         d.xr = gridX[iRight];
-        d.eps_newton = 1e-8;
+        d.eps_newton = config ? config->EpsNewton : 1e-8;  // unused by a shoot; kept for reuse
         d.nl = (int)nl;
         d.nr = (int)nr;
         d.prec_irk = Precision;

@@ -28,7 +28,7 @@ STATUS = ["PCC_OK", "PCC_ERR_INVALID_ARG", "PCC_ERR_CUDA", "PCC_ERR_OOM", "PCC_E
           "PCC_ERR_DELTA_MISMATCH", "PCC_ERR_NAN", "PCC_ERR_LU_SINGULAR", "PCC_ERR_IR_STALL", "PCC_ERR_UNSUPPORTED",
           "PCC_ERR_NEWTON_NO_CONVERGENCE", "PCC_ERR_BUSY", "PCC_ERR_TIMEOUT"]
 PREC_FP64, PREC_MIXED = 0, 1
-PCC_ERR_NAN, PCC_ERR_TIMEOUT = 6, 12
+PCC_ERR_INVALID_ARG, PCC_ERR_NAN, PCC_ERR_BUSY, PCC_ERR_TIMEOUT = 1, 6, 11, 12
 
 # every function include/pcc.h declares
 EXPORTS = ["pcc_ctx_create", "pcc_ctx_destroy", "pcc_status_string", "pcc_last_error", "pcc_solve_create",

@@ -7,7 +7,8 @@ input and exits (one iteration cannot meet PrecisionNewton = 1e-30).
 
 Output: tests/golden/ref_debug_128.npz: the snapshot keys (std::to_string of
 x), the A/U/V/f arrays per key, the Jacobian, and the input configuration.
-Needs oracle/_ref/cc_openmp (oracle/build_ref.sh).
+Needs oracle/_ref/cc_openmp (oracle/build_ref.sh) and the reference tree
+(PCC_REFERENCE_ROOT=<checkout>, for data/simulation_4D_128.json).
 """
 import json
 import os
@@ -20,11 +21,19 @@ import numpy as np
 HERE = pathlib.Path(__file__).resolve().parent
 REPO = HERE.parent.parent
 CC = REPO / "oracle" / "_ref" / "cc_openmp"
-FIXTURE = pathlib.Path("/root/reference/data/simulation_4D_128.json")
+
+
+def fixture_path():
+    import sys
+
+    sys.path.insert(0, str(HERE))
+    from ref_lib import reference_root
+
+    return reference_root() / "data" / "simulation_4D_128.json"
 
 
 def main():
-    cfg = json.loads(FIXTURE.read_text())
+    cfg = json.loads(fixture_path().read_text())
     cfg.update({"NLeft": 1000, "NRight": 1000, "PrecisionNewton": 1e-30, "MaxIterNewton": 1, "Verbose": False,
                 "Debug": True, "DebugNx": 100, "DebugNtau": 4, "Converged": False})
     with tempfile.TemporaryDirectory() as tmp:

@@ -2,7 +2,9 @@
 
 TEST INFRASTRUCTURE ONLY.  Run where the reference tree exists:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference checkout> [--cases c1 c2 ...]
+
+(--reference defaults to $PCC_REFERENCE_ROOT.)
 
 Sources of truth:
   * test/test_init_gen.cpp (the reference's own golden vectors, parsed as text)
@@ -17,9 +19,21 @@ the grid sizes the case uses), the packed Newton input in0 (Delta in slot
 2*Nnewton/3+2), and the reference's outputs: boundary states, RHS
 evaluations, single IRK steps, the base shoot, Jacobian columns and, where
 the full Jacobian is present, the LAPACK Newton update.
+
+Further cases:
+  * c3_seed1024 -- the benchmark's own C3 input (bench.workload(1024, 0.1)):
+    its base shoot and 24 reference Jacobian columns (0..15, 508..515);
+  * c2_newton, c3_newton -- the reference's Newton loop
+    (NewtonSolver.cpp:279-366) from a seeded 1e-3 / 1e-4 relative
+    perturbation of the near-solution until the mismatch RMS is below 1e-12:
+    the first step's Jacobian (C2 only; 4.7 MB at C3 is not committed), LAPACK
+    update and next iterate, the residual/Delta history and the converged
+    unknowns.  The C3 run takes hours on 8 cores; the file is rewritten after
+    every iteration (key `done` = 0 until the loop has ended).
 """
 import argparse
 import json
+import os
 import re
 import sys
 import time
@@ -140,31 +154,108 @@ def newton_to_convergence(R, cfg, in0, name, threads, iters=8):
     print(name, "history", hist)
 
 
+def bench_input_case(R, threads):
+    """The benchmark's C3 input (bench.workload: seed 1024, amplitude 0.1 around
+    the packed near-solution) through the reference: base shoot and Jacobian
+    columns 0..15 (the CPU-baseline sample) and 508..515 (the last f_c modes
+    before and after Delta's slot 514)."""
+    sys.path.insert(0, str(HERE.parents[1]))
+    import bench  # the repository's benchmark: its workload() makes the input
+
+    cfg, in0 = bench.workload(1024, 0.1)
+    t = time.time()
+    out0 = R.shoot(cfg, in0)
+    idx = list(range(16)) + list(range(508, 516))
+    cols = np.concatenate([R.jacobian_columns(cfg, in0, out0, 0, 16, threads),
+                           R.jacobian_columns(cfg, in0, out0, 508, 516, threads)], axis=1)
+    np.savez_compressed(HERE / "ref_c3_seed1024.npz", config=json.dumps(cfg), seed=1024, amp=0.1, in0=in0,
+                        out0=out0, jac_idx=np.array(idx), jac_cols=cols, t_s=time.time() - t)
+    print("c3_seed1024", cols.shape, f"{time.time() - t:.0f} s")
+
+
+def newton_case(R, cfg, x0, name, threads, store_jacobian, tol=1e-12, max_iters=8):
+    """The reference's Newton loop (NewtonSolver.cpp:279-366, which stops when
+    the mismatch RMS drops below PrecisionNewton; here `tol`) from x0, with a
+    checkpoint after every iteration."""
+    nn = x0.size
+    islot = 2 * nn // 3 + 2
+    base = {"config": json.dumps({k: v for k, v in cfg.items() if k != "Initial_Conditions"}), "in0": x0,
+            "tol": tol}
+    x = x0.copy()
+    hist, extra = [], {}
+    t0 = time.time()
+    for it in range(max_iters):
+        out = R.shoot(cfg, x)
+        err = float(np.sqrt(np.mean(out ** 2)))
+        hist.append([err, x[islot]])
+        if it == 0:
+            extra["out0"] = out
+        elif it == 1:
+            extra["newton_out1"] = out
+        if err < tol:
+            break
+        J = R.jacobian_columns(cfg, x, out, 0, nn, threads)
+        dx = R.solve(J, -out)
+        fac = min(1.0, cfg["SlowError"] / err)
+        if it == 0:
+            extra.update(newton_dx=dx, newton_in1=x + fac * dx, newton_err=err)
+            if store_jacobian:
+                extra["jacobian"] = J
+        x = x + fac * dx
+        np.savez_compressed(HERE / f"ref_{name}.npz", **base, **extra, x_last=x, history=np.array(hist), done=0,
+                            t_s=time.time() - t0)
+        print(name, "iteration", it, "err", err, "Delta", hist[-1][1], f"{time.time() - t0:.0f} s", flush=True)
+    np.savez_compressed(HERE / f"ref_{name}.npz", **base, **extra, x_star=x, history=np.array(hist), done=1,
+                        t_s=time.time() - t0)
+    print(name, "history", hist, flush=True)
+
+
+CASES = ["init_gen", "c1", "c2", "c3", "c3_seed1024", "c2_newton", "c3_newton"]
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("PCC_REFERENCE_ROOT"),
+                    help="reference checkout (default $PCC_REFERENCE_ROOT)")
     ap.add_argument("--threads", type=int, default=8)
+    ap.add_argument("--cases", nargs="+", choices=CASES, default=CASES[:5])
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("give --reference or set PCC_REFERENCE_ROOT")
     ref = Path(a.reference)
-    src = (ref / "test" / "test_init_gen.cpp").read_text()
-    g = parse_init_gen(src)
-    np.savez_compressed(HERE / "init_gen_128.npz", ntau=128, dim=4.0, delta=3.445501184653556, xl=0.001, xr=0.999,
-                        **g)
+    if "init_gen" in a.cases:
+        src = (ref / "test" / "test_init_gen.cpp").read_text()
+        g = parse_init_gen(src)
+        np.savez_compressed(HERE / "init_gen_128.npz", ntau=128, dim=4.0, delta=3.445501184653556, xl=0.001,
+                            xr=0.999, **g)
     R = RefLib()
     rng = np.random.default_rng(SEED)
-    # C1: Ntau=128, 1000+1000 points, full Jacobian and Newton step, fixture and seeded perturbation
-    cfg = config(ref, 128, 1000, 1000)
-    z = packed_input(R, cfg)
-    case(R, cfg, z, "c1_fixture", range(96), a.threads, full_newton=True)
-    zp = perturb(z, 1e-3, rng)
-    case(R, cfg, zp, "c1_perturbed", range(96), a.threads, full_newton=True)
-    newton_to_convergence(R, cfg, zp, "c1_newton", a.threads)
-    # C2: Ntau=512, 3000+3000: base shoot and the leading column of each field plus Delta
-    cfg = config(ref, 512, 3000, 3000)
-    case(R, cfg, packed_input(R, cfg), "c2_fixture", [0, 128, 256, 258], a.threads)
-    # C3: Ntau=1024, 4000+4000: the same columns (Up mode 1, psi_c mode 1, f_c DC, Delta)
-    cfg = config(ref, 1024, 4000, 4000)
-    case(R, cfg, packed_input(R, cfg), "c3_fixture", [0, 256, 512, 514], a.threads)
+    if "c1" in a.cases:
+        # C1: Ntau=128, 1000+1000 points, full Jacobian and Newton step, fixture and seeded perturbation
+        cfg = config(ref, 128, 1000, 1000)
+        z = packed_input(R, cfg)
+        case(R, cfg, z, "c1_fixture", range(96), a.threads, full_newton=True)
+        zp = perturb(z, 1e-3, rng)
+        case(R, cfg, zp, "c1_perturbed", range(96), a.threads, full_newton=True)
+        newton_to_convergence(R, cfg, zp, "c1_newton", a.threads)
+    if "c2" in a.cases:
+        # C2: Ntau=512, 3000+3000: base shoot and the leading column of each field plus Delta
+        cfg = config(ref, 512, 3000, 3000)
+        case(R, cfg, packed_input(R, cfg), "c2_fixture", [0, 128, 256, 258], a.threads)
+    if "c3" in a.cases:
+        # C3: Ntau=1024, 4000+4000: the same columns (Up mode 1, psi_c mode 1, f_c DC, Delta)
+        cfg = config(ref, 1024, 4000, 4000)
+        case(R, cfg, packed_input(R, cfg), "c3_fixture", [0, 256, 512, 514], a.threads)
+    if "c3_seed1024" in a.cases:
+        bench_input_case(R, a.threads)
+    if "c2_newton" in a.cases:
+        cfg = config(ref, 512, 3000, 3000)
+        z = perturb(packed_input(R, cfg), 1e-3, np.random.default_rng(SEED + 2))
+        newton_case(R, cfg, z, "c2_newton", a.threads, store_jacobian=True)
+    if "c3_newton" in a.cases:
+        cfg = config(ref, 1024, 4000, 4000)
+        z = perturb(packed_input(R, cfg), 1e-4, np.random.default_rng(SEED + 3))
+        newton_case(R, cfg, z, "c3_newton", a.threads, store_jacobian=False)
 
 
 if __name__ == "__main__":

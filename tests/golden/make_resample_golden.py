@@ -4,19 +4,23 @@ applied to the Ntau = 128 near-solution fields of data/simulation_4D_128.json,
 doubled three times (128 -> 256 -> 512 -> 1024).
 
 Output: tests/golden/ref_resample_128.npz with the input fields and every
-doubling.  Runs in the development container (the reference tree is needed).
+doubling.  Needs the reference tree: PCC_REFERENCE_ROOT=<checkout>.
 """
 import importlib.util
 import json
 import pathlib
 
+import sys
+
 import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
-REF = pathlib.Path("/root/reference")
+sys.path.insert(0, str(HERE))
+from ref_lib import reference_root  # noqa: E402
 
 
 def main():
+    REF = reference_root()
     spec = importlib.util.spec_from_file_location("create_simulation_data",
                                                   REF / "scripts" / "create_simulation_data.py")
     mod = importlib.util.module_from_spec(spec)

@@ -18,7 +18,8 @@ floor of this map (its Newton loop stalls near 1e-13 and then exits).
 
 Output: tests/golden/ref_suite_128.npz with, per branch, the ordered dimension
 keys, Delta, fc, psic, Up, Converged and IterNewton as the reference wrote them,
-plus the suite input.  Needs oracle/_ref/cc_openmp (oracle/build_ref.sh).
+plus the suite input.  Needs oracle/_ref/cc_openmp (oracle/build_ref.sh) and the reference tree
+(PCC_REFERENCE_ROOT=<checkout>, for data/simulation_4D_128.json).
 """
 import json
 import os
@@ -32,7 +33,15 @@ import numpy as np
 HERE = pathlib.Path(__file__).resolve().parent
 REPO = HERE.parent.parent
 CC = REPO / "oracle" / "_ref" / "cc_openmp"
-FIXTURE = pathlib.Path("/root/reference/data/simulation_4D_128.json")
+
+
+def fixture_path():
+    import sys
+
+    sys.path.insert(0, str(HERE))
+    from ref_lib import reference_root
+
+    return reference_root() / "data" / "simulation_4D_128.json"
 STEP = 0.01
 
 
@@ -51,7 +60,7 @@ def suite(dims, seed_cfg):
 
 
 def main():
-    base = json.loads(FIXTURE.read_text())
+    base = json.loads(fixture_path().read_text())
     base.update({"NLeft": 1000, "NRight": 1000, "PrecisionNewton": 1e-12, "MaxIterNewton": 20,
                  "Verbose": False, "Debug": False})
     up = [4.0 + STEP * i for i in range(5)]         # 4.00 .. 4.04

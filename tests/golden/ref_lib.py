@@ -125,3 +125,12 @@ class RefLib:
 
 def available():
     return REF_SO.exists()
+
+
+def reference_root():
+    """The reference checkout the fixture scripts read (data/, test/, scripts/):
+    $PCC_REFERENCE_ROOT, which they require."""
+    root = os.environ.get("PCC_REFERENCE_ROOT")
+    if not root or not Path(root, "src").is_dir():
+        raise SystemExit("set PCC_REFERENCE_ROOT to the reference checkout (the directory holding src/ and data/)")
+    return Path(root)

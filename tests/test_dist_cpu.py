@@ -71,3 +71,23 @@ def test_column_blocks_cover_every_column():
             b = bench.column_blocks(nn, world)
             assert len(b) == world and b[0][0] == 0 and b[-1][1] == nn
             assert all(b[i][1] == b[i + 1][0] for i in range(world - 1))
+
+
+def test_bench_launches_its_own_ranks_dry_run():
+    """`bench.py --gpus 2` with no outer launcher starts two ranks itself
+    (torch.distributed.run, 127.0.0.1); with --dry-run they run the column
+    partition, the all-gather and the max-over-ranks reduction on gloo, and
+    rank 0 alone prints one line with n_gpus = 2."""
+    import json
+    import subprocess
+
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, str(REPO / "bench.py"), "--gpus", "2", "--dry-run", "--steps", "1",
+                        "--warmup", "0"], capture_output=True, text=True, timeout=300, env=env, cwd=str(REPO))
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    line = lines[0]
+    assert line["dry_run"] and line["n_gpus"] == 2 and line["gather_ok"]
+    assert line["blocks"] == [[0, 384], [384, 768]] and line["max_over_ranks"] == 2.0
+    assert line["config"]["parallelism"] == "2 independent solves, one per GPU"

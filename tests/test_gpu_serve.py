@@ -136,3 +136,52 @@ def test_serve_wait_times_out_and_rejects_non_finite_input(engine):
         assert e.value.status == pcc.PCC_ERR_NAN
     finally:
         engine.serve_stop()
+
+
+def test_serve_stop_while_waiting_and_results_delivered_once(engine):
+    """pcc_serve_stop overlapping a pcc_wait and a pcc_poll loop on other
+    threads: the waiter still receives its result (stop finishes every
+    submitted request first), the poller ends with PCC_ERR_INVALID_ARG once the
+    server is gone, and nothing blocks.  A delivered result is released: the
+    ticket is unknown afterwards."""
+    import ctypes
+    import threading
+
+    import pcc
+
+    c1 = load_case("c1_newton")
+    cfg = _cfg(c1, PrecisionNewton=1e-12, MaxIterNewton=12)
+    engine.serve_start()
+    t_done = engine.submit(cfg, c1["in0"])
+    r, _ = engine.wait(t_done)
+    assert r["done"] == 1
+    with pytest.raises(pcc.PccError) as e:
+        engine.poll(t_done)  # delivered once
+    assert e.value.status == pcc.PCC_ERR_INVALID_ARG
+
+    t = engine.submit(cfg, c1["in0"])
+    got, polled = {}, {}
+
+    def waiter():
+        got["r"], got["x"] = engine.wait(t, 600.0)
+
+    def poller():
+        res = pcc.Result()
+        codes = set()
+        while not got.get("stopped"):
+            codes.add(engine.lib.pcc_poll(engine.ctx, ctypes.c_uint64(t + 1000), ctypes.byref(res), None))
+            time.sleep(0.001)
+        codes.add(engine.lib.pcc_poll(engine.ctx, ctypes.c_uint64(t + 1000), ctypes.byref(res), None))
+        polled["codes"] = codes
+
+    th_w, th_p = threading.Thread(target=waiter), threading.Thread(target=poller)
+    th_w.start()
+    th_p.start()
+    time.sleep(0.05)
+    engine.serve_stop()
+    got["stopped"] = True
+    th_w.join(60)
+    th_p.join(60)
+    assert not th_w.is_alive() and not th_p.is_alive()
+    assert got["r"]["done"] == 1 and got["r"]["status"] == 0 and got["x"] is not None
+    assert polled["codes"] <= {pcc.PCC_ERR_INVALID_ARG}  # unknown ticket before and after the stop

@@ -21,6 +21,27 @@ from conftest import load_case
 pytestmark = pytest.mark.gpu
 
 
+def _interp_field(f, n):
+    """Spectral (zero-padding) interpolation of a periodic real field to n samples."""
+    c = np.fft.rfft(f)
+    c2 = np.zeros(n // 2 + 1, dtype=complex)
+    c2[: c.size - 1] = c[:-1]
+    return np.fft.irfft(c2, n) * (n / f.size)
+
+
+def _cases():
+    """The C1 and C3 fixtures, and the C1 fields interpolated to Ntau 2048: the
+    largest size the static work area holds, which fills it exactly."""
+    for name in ["c1_fixture", "c3_fixture"]:
+        d = load_case(name)
+        n = d["cfg"]["Ntau"]
+        yield name, d["cfg"], float(d["in0"][2 * (3 * n // 4) // 3 + 2]), d["unpack_fc"], d["unpack_psic"], \
+            d["unpack_up"]
+    d = load_case("c1_fixture")
+    fc, psic, up = (_interp_field(d[k], 2048) for k in ("unpack_fc", "unpack_psic", "unpack_up"))
+    yield "c1_at_2048", dict(d["cfg"], Ntau=2048), float(d["in0"][2 * d["in0"].size // 3 + 2]), fc, psic, up
+
+
 def test_static_expansions_match_allocating_entry_point(engine):
     import torch
 
@@ -28,12 +49,8 @@ def test_static_expansions_match_allocating_entry_point(engine):
 
     lib = pcc.load()
     dev = torch.device("cuda", 0)
-    for name in ["c1_fixture", "c3_fixture"]:
-        d = load_case(name)
-        cfg = d["cfg"]
+    for name, cfg, delta, fc, psic, up in _cases():
         n = cfg["Ntau"]
-        delta = float(d["in0"][2 * (3 * n // 4) // 3 + 2])
-        fc, psic, up = d["unpack_fc"], d["unpack_psic"], d["unpack_up"]
         yl_ref, yr_ref = engine.expansions(n, cfg["Dim"], delta, cfg["XLeft"], cfg["XRight"], fc, psic, up)
         t_fc, t_ps, t_up = (torch.tensor(a, dtype=torch.float64, device=dev) for a in (fc, psic, up))
         for call in range(2):
@@ -49,6 +66,7 @@ def test_static_expansions_match_allocating_entry_point(engine):
             yl, yr = t_yl.cpu().numpy(), t_yr.cpu().numpy()
             assert np.max(np.abs(yl - yl_ref)) / np.max(np.abs(yl_ref)) < 1e-12, (name, call)
             assert np.max(np.abs(yr - yr_ref)) / np.max(np.abs(yr_ref)) < 1e-12, (name, call)
+    assert torch.cuda.current_device() == 0  # the caller's current device is left as it was
 
 
 def test_static_expansions_rejects_oversize(engine):
