@@ -451,11 +451,31 @@ def newton_compare(eng, cfg, in0, out0, J):
         s.jacobian_columns(in0, out0, c, c + 1)
     per_col = (time.perf_counter() - t) / sample
     b = -np.asarray(out0)
+    for prec in (pcc.PREC_FP64, pcc.PREC_MIXED):
+        eng.lu_solve(J, b, precision=prec)  # first calls set the kernels' shared-memory limits
     t = time.perf_counter()
-    x64, _ = eng.lu_solve(J, b, precision=pcc.PREC_FP64)
+    x64, rep64 = eng.lu_solve(J, b, precision=pcc.PREC_FP64)
     lu_ms = (time.perf_counter() - t) * 1e3
     xm, rep = eng.lu_solve(J, b, precision=pcc.PREC_MIXED)
+    old_tc = os.environ.get("PCC_LU_TC")
+    os.environ["PCC_LU_TC"] = "0"
+    eng.lu_solve(J, b, precision=pcc.PREC_MIXED)
+    xc, repc = eng.lu_solve(J, b, precision=pcc.PREC_MIXED)
+    if old_tc is None:
+        os.environ.pop("PCC_LU_TC")
+    else:
+        os.environ["PCC_LU_TC"] = old_tc
     x_lapack = np.linalg.solve(J, b)  # LAPACK dgesv (numpy)
+    out["lu"] = {"n": nn, "ms_fp64": rep64["ms"], "ms_mixed_tensor_cores": rep["ms"],
+                 "ms_mixed_cuda_cores": repc["ms"], "refinement_steps": rep["refinement_steps"],
+                 "fell_back_to_fp64": rep["fell_back_to_fp64"],
+                 "mixed_tc_dx_rel_err_vs_lapack_dgesv": float(np.linalg.norm(xm - x_lapack) /
+                                                              np.linalg.norm(x_lapack)),
+                 "mixed_cuda_cores_dx_rel_err_vs_lapack_dgesv": float(np.linalg.norm(xc - x_lapack) /
+                                                                      np.linalg.norm(x_lapack)),
+                 "what": "device time of one solve (factorisation, solve, refinement) on the timed build's J; "
+                         "mixed = FP32 LU (trailing updates on tcgen05 TF32 high/low, or on the CUDA cores) "
+                         "+ FP64 refinement"}
     out["ms_plain_fp64"] = per_col * (nn + 1) * 1e3 + lu_ms
     out["plain_form"] = (f"one march launch per shoot (base + {nn} columns); {sample} columns timed, "
                          f"extrapolated; FP64 LU {lu_ms:.1f} ms")
@@ -471,8 +491,10 @@ def newton_compare(eng, cfg, in0, out0, J):
 def run_dscan(eng, args):
     """C4: 16 solves, D = 3.25, 3.35, .., 4.75, Ntau drawn from {128, 256, 512,
     1024} and points from {2000, 4000, 6000, 8000} (seeded; at least
-    MIN_POINTS[Ntau]), seeded free data, one Newton iteration of all 16 in one
-    batch launch (mixed-precision solve)."""
+    MIN_POINTS[Ntau]), seeded free data, batched: one Newton iteration of all
+    16 in one batch launch timed alone (Jacobian builds/s), then all 16 to
+    convergence (NewtonSolver::run for each, every iteration's shoots of every
+    running solve in one launch, mixed-precision solve)."""
     import pcc
 
     if not SEEDS.exists():
@@ -482,7 +504,7 @@ def run_dscan(eng, args):
     dims = 3.25 + 0.1 * np.arange(16)
     ns = rng.choice([128, 256, 512, 1024], 16)
     pts = [int(rng.choice([p for p in (2000, 4000, 6000, 8000) if p >= MIN_POINTS[int(n)]])) for n in ns]
-    solves, xs, rejects = [], [], []
+    solves, xs, rejects, cfgs = [], [], [], []
     for d, n, p in zip(dims, ns, pts):
         for attempt in range(4):
             cfg, z = seed_request(eng, seeds, d, int(n), int(p))
@@ -498,6 +520,7 @@ def run_dscan(eng, args):
         if s is not None:
             solves.append(s)
             xs.append(z)
+            cfgs.append(cfg)
     for s, z in zip(solves, xs):  # warm-up iteration
         s.newton_begin(z)
     eng.newton_iterate(solves, precision=pcc.PREC_MIXED)
@@ -505,26 +528,34 @@ def run_dscan(eng, args):
         s.newton_begin(z)
     st = pcc.Stats()
     t = time.perf_counter()
-    states = eng.newton_iterate(solves, precision=pcc.PREC_MIXED, stats=st)
+    eng.newton_iterate(solves, precision=pcc.PREC_MIXED, stats=st)
     wall = time.perf_counter() - t
-    out = {"solves": len(solves), "rejected_draws": rejects,
-           "ntau": [int(s.ntau) for s in solves], "points": [int(s.desc.nl + s.desc.nr) for s in solves],
-           "dims": [float(s.desc.dim) for s in solves], "wall_s": wall,
-           "jacobian_builds_per_s": len(solves) / wall, "ms_batch_march": st.ms_sweep,
-           "rhs_evals": st.rhs_evals, "sweeps": int(st.shoots) * 2,
-           "states": [x["state"] for x in states], "free_data_amp": args.dscan_amp,
-           "lu": "mixed (FP32 LU + FP64 refinement)"}
     for s in solves:
         s.close()
-    return out
+    # the same 16 solves to convergence
+    tol = 1e-10
+    conv = [eng.solve(dict(c, PrecisionNewton=tol, MaxIterNewton=args.dscan_iters)) for c in cfgs]
+    t = time.perf_counter()
+    x_out, states = eng.newton_solve(conv, xs, precision=pcc.PREC_MIXED)
+    wall_conv = time.perf_counter() - t
+    for s in conv:
+        s.close()
+    return {"solves": len(solves), "rejected_draws": rejects,
+            "ntau": [int(c["Ntau"]) for c in cfgs], "points": [int(c["NLeft"] + c["NRight"]) for c in cfgs],
+            "dims_requested": [float(d) for d in dims], "dims": [float(c["Dim"]) for c in cfgs],
+            "wall_s": wall, "jacobian_builds_per_s": len(solves) / wall, "ms_batch_march": st.ms_sweep,
+            "rhs_evals": st.rhs_evals, "sweeps": int(st.shoots) * 2,
+            "converge": {"tolerance": tol, "max_iterations": args.dscan_iters, "wall_s": wall_conv,
+                         "states": [x["state"] for x in states], "iterations": [x["iterations"] for x in states],
+                         "err": [x["err"] for x in states],
+                         "delta": [float(x[2 * x.size // 3 + 2]) for x in x_out]},
+            "free_data_amp": args.dscan_amp, "lu": "mixed (FP32 LU on tensor cores + FP64 refinement)"}
 
 
-def run_serving(eng, args, rate, n_req):
-    """C5: a seeded Poisson stream of whole Newton solves, D ~ U[3.25, 4.75] (on
-    the 0.01 grid of the seed table), Ntau from {128, 256, 512, 1024}, points
-    ~ U[MIN_POINTS[Ntau], 8000]; latency = submit -> result (host clock)."""
-    if not SEEDS.exists():
-        return {"unavailable": "bench_data/dscan_seeds_128.npz missing (bench_data/make_dscan_seeds.py)"}
+def serving_requests(eng, args, n_req):
+    """C5's seeded request stream: D ~ U[3.25, 4.75] (the nearest dimension of
+    the seed table, 0.01 apart), Ntau from {128, 256, 512, 1024}, points ~
+    U[MIN_POINTS[Ntau], 8000] (even)."""
     seeds = np.load(SEEDS)
     rng = np.random.default_rng(args.seed + 5)
     reqs = []
@@ -534,29 +565,49 @@ def run_serving(eng, args, rate, n_req):
         p = 2 * int(rng.integers(MIN_POINTS[n] // 2, 4001))
         cfg, z = seed_request(eng, seeds, d, n, p)
         cfg.update({"PrecisionNewton": 1e-10, "MaxIterNewton": 10})
-        reqs.append((cfg, z))
+        reqs.append((cfg, z, d))
+    return reqs, rng
+
+
+def run_serving(eng, args, rate, n_req, precision="fp64"):
+    """C5 at one arrival rate: a seeded Poisson stream of whole Newton solves;
+    latency = submit -> result (host clock), service = latency minus the time
+    queued before admission."""
+    import pcc
+
+    if not SEEDS.exists():
+        return {"unavailable": "bench_data/dscan_seeds_128.npz missing (bench_data/make_dscan_seeds.py)"}
+    reqs, rng = serving_requests(eng, args, n_req)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    prec = pcc.PREC_MIXED if precision == "mixed" else pcc.PREC_FP64
     eng.serve_start()
     t0 = time.perf_counter()
     tickets = []
-    for (cfg, z), a in zip(reqs, arrivals):
+    for (cfg, z, _), a in zip(reqs, arrivals):
         dt = t0 + a - time.perf_counter()
         if dt > 0:
             time.sleep(dt)
-        tickets.append(eng.submit(cfg, z))
+        tickets.append(eng.submit(cfg, z, precision=prec))
     res = [eng.wait(t, 3600.0)[0] for t in tickets]
     span = time.perf_counter() - t0
     info = eng.serve_stats()
     eng.serve_stop()
     lat = np.array([r["ms_latency"] for r in res])
-    return {"rate_per_s": rate, "requests": n_req, "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+    svc = np.array([r["ms_latency"] - r["ms_queued"] for r in res])
+    q = np.array([r["ms_queued"] for r in res])
+    return {"rate_per_s": rate, "requests": n_req, "precision": precision,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "service_p50_ms": float(np.percentile(svc, 50)),
+            "service_p99_ms": float(np.percentile(svc, 99)), "queued_p50_ms": float(np.percentile(q, 50)),
+            "queued_p99_ms": float(np.percentile(q, 99)),
             "throughput_solves_per_s": n_req / span, "span_s": span,
             "converged": int(sum(r["newton"]["state"] == "CONVERGED" for r in res)),
-            "statuses": [r["status_name"] for r in res],
-            "iterations": [r["newton"]["iterations"] for r in res],
-            "ntau": [c["Ntau"] for c, _ in reqs], "launches": info["launches"], "sweeps": info["sweeps"],
-            "precision": "fp64", "newton_tolerance": 1e-10}
+            "statuses": sorted(set(r["status_name"] for r in res)),
+            "iterations_mean": float(np.mean([r["newton"]["iterations"] for r in res])),
+            "ntau": [c["Ntau"] for c, _, _ in reqs], "dims_requested": [float(d) for _, _, d in reqs],
+            "dims": [float(c["Dim"]) for c, _, _ in reqs], "launches": info["launches"],
+            "sweeps": info["sweeps"], "newton_tolerance": 1e-10,
+            "note": "percentiles over `requests` draws (with 16 the p99 is the maximum)"}
 
 
 def run_engine(args, world, rank, local):
@@ -652,7 +703,11 @@ def run_engine(args, world, rank, local):
     predictor = predictor_build(eng, cfg, in0, out0, h_J.numpy().copy(), args.steps, flush) if extras else None
     newton = newton_compare(eng, cfg, in0, out0, h_J.numpy().copy()) if extras else None
     dscan = run_dscan(eng, args) if extras else None
-    serving = run_serving(eng, args, args.rate, args.requests) if extras else None
+    serving = None
+    if extras:
+        serving = [run_serving(eng, args, float(r), args.requests) for r in args.rates.split(",") if r]
+        serving += [run_serving(eng, args, float(r), args.requests, "mixed") for r in args.mixed_rates.split(",")
+                    if r]
 
     cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -693,8 +748,11 @@ def main():
     ap.add_argument("--amp", type=float, default=0.1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--quick", action="store_true", help="only the Jacobian build line (no Newton/C4/C5 sections)")
-    ap.add_argument("--rate", type=float, default=4.0, help="C5 Poisson arrival rate (requests/s)")
-    ap.add_argument("--requests", type=int, default=16, help="C5 requests")
+    ap.add_argument("--rates", default="0.25,1,4,16",
+                    help="C5 Poisson arrival rates (requests/s), FP64 Newton solves; 0.25 is below capacity")
+    ap.add_argument("--mixed-rates", default="4", help="C5 rates served again with the mixed-precision solve")
+    ap.add_argument("--requests", type=int, default=16, help="C5 requests per rate")
+    ap.add_argument("--dscan-iters", type=int, default=20, help="C4: Newton iteration cap of the convergence run")
     ap.add_argument("--dscan-amp", type=float, default=0.01, help="C4 free-data perturbation amplitude")
     ap.add_argument("--shard", choices=["solves", "columns"], default="solves",
                     help="multi-GPU: independent solves per GPU (weak scaling, default) or one Jacobian's "

@@ -149,7 +149,13 @@ pcc_status pcc_jacobian_columns(pcc_solve* s, const double* in0, const double* o
                                 double* cols, pcc_stats* stats);
 
 /* NewtonSolver::solveLinearSystem (NewtonSolver.cpp:739-757): A x = rhs,
- * A row-major n x n.  FP64 LU, or FP32 LU refined to FP64. */
+ * A row-major n x n, n <= 3128 (a factorisation panel of n rows lives in
+ * shared memory; every Newton system here has n = 3 Ntau / 4 <= 1536).  FP64
+ * LU (LAPACKE_dgesv semantics), or PCC_PREC_MIXED: an FP32 LU whose trailing
+ * updates run on the tensor cores (TF32 with a high/low split of each FP32
+ * operand, FP32 accumulation; $PCC_LU_TC=0 keeps them on the CUDA cores),
+ * refined to FP64 with FP64 residuals as LAPACK dsgesv does, falling back to
+ * the FP64 LU if the refinement does not converge in 30 sweeps. */
 pcc_status pcc_lu_solve(pcc_ctx* ctx, int n, const double* A, const double* rhs, double* x, pcc_precision prec,
                         pcc_refine_report* report);
 
@@ -333,12 +339,14 @@ pcc_status pcc_resample_fields(pcc_ctx* ctx, int ntau_in, int ntau_out, int coun
 /* The IRK march kernel's transform schedule for (Ntau, stages) on the
  * context's device, picked by this library's autotuner (no counterpart in the
  * reference): 1 = the independent transforms of an RHS evaluation run in
- * pairs, 0 = one at a time.  The first solve of a shape times both on a short
- * single-RHS probe, keeps pairs unless one at a time is more than 3 % faster,
- * and caches the choice ($PCC_AUTOTUNE_CACHE, default
- * ~/.cache/pcc_b200/autotune.txt; $PCC_AUTOTUNE=0 keeps pairs); this call
- * tunes now if needed.  ms_pair/ms_single: probe times, 0 when read from the
- * cache. */
+ * pairs, 0 = one at a time, 2 (Ntau 1024, 2 stages) = pairs of length-512
+ * transforms with one of their two data exchanges inside a warp.  The first
+ * solve of a shape times the schedules on a short single-RHS probe, keeps
+ * pairs unless another schedule is more than 3 % faster, and caches the
+ * choice ($PCC_AUTOTUNE_CACHE, default ~/.cache/pcc_b200/autotune.txt;
+ * $PCC_AUTOTUNE=0 keeps pairs; $PCC_MARCH_SCHEDULE=0|1|2 forces a schedule
+ * wherever the shape has it); this call tunes now if needed.
+ * ms_pair/ms_single: probe times, 0 when read from the cache. */
 pcc_status pcc_march_tuning(pcc_ctx* ctx, int ntau, int stages, int* pair, double* ms_pair, double* ms_single);
 
 /* Replaces the solve's x-grid (NewtonSolver::generateGrid output) by grid,

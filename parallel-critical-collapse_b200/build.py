@@ -43,6 +43,7 @@ def _units():
         for pair in (0, 1):
             units.append((CSRC / "march.cu", OBJ / f"march_n{n}_p{pair}.o",
                           [f"-DPCC_MARCH_N={n}", f"-DPCC_MARCH_PAIR={pair}"]))
+    units.append((CSRC / "march.cu", OBJ / "march_n1024_p2.o", ["-DPCC_MARCH_N=1024", "-DPCC_MARCH_PAIR=2"]))
     units.append((CSRC / "march.cu", OBJ / "march_dispatch.o", ["-DPCC_MARCH_DISPATCH"]))
     units.append((CSRC / "march.cu", OBJ / "march_batch.o", ["-DPCC_MARCH_BATCH"]))
     for name in ["boundary", "lu", "newton", "pcc_abi", "resample", "serve", "static_scratch"]:

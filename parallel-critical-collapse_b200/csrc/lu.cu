@@ -2,17 +2,34 @@
 // NewtonSolver.cpp:739-757, which calls LAPACKE_dgesv on the row-major J).
 //
 // Blocked right-looking LU with partial pivoting on a row-major matrix, the
-// algorithm of LAPACK dgetrf/dgetrs: per panel of NB columns a single-CTA
-// panel factorisation (pivot = first entry of maximal modulus, as idamax; the
-// whole row is swapped; multipliers scaled by the reciprocal pivot as dgetf2
-// does), a triangular solve for the U12 block row, and a tiled rank-NB update
-// of the trailing matrix spread over the GPU.  Templated on the working type:
-// FP64 for the reference-equivalent solve, FP32 for the mixed-precision solve,
-// which is refined to FP64 accuracy with FP64 residuals as LAPACK dsgesv does
-// (stop when ||r||_inf <= sqrt(n) eps ||A||_inf ||x||_inf, at most 30 sweeps,
-// else fall back to the FP64 factorisation).
+// algorithm of LAPACK dgetrf/dgetrs.  Per panel of NB columns:
+//   panel_kernel      the panel factorisation in shared memory (one CTA):
+//                     pivot = first entry of maximal modulus (idamax), the
+//                     panel rows swapped, multipliers scaled by the
+//                     reciprocal pivot (dgetf2), rank-1 updates of the panel;
+//   swap_trsm_kernel  the panel's row interchanges applied to every other
+//                     column (dlaswp) and U12 = L11^{-1} A12 (dtrsm), one
+//                     thread per column;
+//   update            A22 -= L21 U12: FP64 on the CUDA cores (update_kernel),
+//                     FP32 on the tensor cores (tc_update_kernel, tcgen05
+//                     kind::tf32 with the FP32 operands split into a TF32 high
+//                     and low part: hi*hi + hi*lo + lo*hi accumulated in FP32
+//                     in Tensor Memory, which keeps FP32 accuracy).
+// The solve with the factors (dgetrs) is one CTA: row swaps, then unit-lower
+// forward and upper backward substitution in blocks of 32 (one warp solves a
+// diagonal block with shuffles, the CTA updates the other rows).
+//
+// Mixed precision = the FP32 factorisation + FP64 residual refinement with
+// LAPACK dsgesv's rule (stop when ||r||_inf <= sqrt(n) eps ||A||_inf
+// ||x||_inf, at most 30 sweeps, else fall back to the FP64 factorisation).
+// The refinement sweeps are enqueued back to back: a device flag set by the
+// convergence check makes the remaining sweeps' kernels return at once, so
+// the host reads the outcome once per chunk of three sweeps (once per solve
+// when it converges within them) instead of once per sweep.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "pcc_internal.h"
@@ -21,96 +38,142 @@ namespace pcc {
 
 namespace {
 
-constexpr int kNB = 32;
+constexpr int kPanelThreads = 512;
+constexpr int kMaxNB = 32;
+constexpr size_t kPanelSmemCap = 220 * 1024;
+
+// Panel width for an n x n matrix of elements of es bytes: the panel's rows
+// (n of them, padded to NB + 1 entries) must fit in shared memory.
+int panel_nb(int n, size_t es)
+{
+    int nb = kMaxNB;
+    while (nb > 8 && (size_t)n * (nb + 1) * es > kPanelSmemCap) nb /= 2;
+    return nb;
+}
 
 template <typename T>
-__global__ void __launch_bounds__(256) panel_kernel(T* A, int n, int k0, int nb, int* ipiv, int* info)
+__global__ void __launch_bounds__(kPanelThreads) panel_kernel(T* A, int n, int k0, int nb, int* ipiv, int* info)
 {
-    __shared__ T smax[256];
-    __shared__ int sidx[256];
-    __shared__ T piv_s;
-    __shared__ int p_s;
-    const int tid = threadIdx.x;
-    const int kend = min(k0 + nb, n);
-    for (int j = k0; j < kend; ++j) {
-        // pivot: first row of maximal |A[i][j]|, i >= j
-        T best = -1;
+    extern __shared__ __align__(16) unsigned char panel_smem[];
+    T* P = reinterpret_cast<T*>(panel_smem);  // [m][nb + 1]
+    constexpr int NW = kPanelThreads / 32;
+    __shared__ T s_val[NW];
+    __shared__ int s_idx[NW];
+    const int m = n - k0, ld = nb + 1, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < m * nb; e += kPanelThreads) {
+        const int r = e / nb, c = e - r * nb;
+        P[r * ld + c] = A[(size_t)(k0 + r) * n + k0 + c];
+    }
+    __syncthreads();
+    for (int j = 0; j < nb && j < m; ++j) {
+        // pivot: the first row of maximal |P[r][j]|, r >= j
+        T best = T(-1);
         int bi = j;
-        for (int i = j + tid; i < n; i += blockDim.x) {
-            const T v = fabs(A[(size_t)i * n + j]);
+        for (int r = j + tid; r < m; r += kPanelThreads) {
+            const T v = fabs(P[r * ld + j]);
             if (v > best) {
                 best = v;
-                bi = i;
+                bi = r;
             }
         }
-        smax[tid] = best;
-        sidx[tid] = bi;
-        __syncthreads();
-        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-            if (tid < o) {
-                const T a = smax[tid], b = smax[tid + o];
-                const int ia = sidx[tid], ib = sidx[tid + o];
-                if (b > a || (b == a && ib < ia)) {
-                    smax[tid] = b;
-                    sidx[tid] = ib;
-                }
+        for (int o = 16; o > 0; o >>= 1) {
+            const T ov = __shfl_down_sync(0xffffffffu, best, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
             }
-            __syncthreads();
+        }
+        if (lane == 0) {
+            s_val[warp] = best;
+            s_idx[warp] = bi;
+        }
+        __syncthreads();
+        T pb = s_val[0];
+        int p = s_idx[0];
+        for (int w = 1; w < NW; ++w) {
+            const T v = s_val[w];
+            const int i = s_idx[w];
+            if (v > pb || (v == pb && i < p)) {
+                pb = v;
+                p = i;
+            }
+        }
+        if (p != j && tid < nb) {
+            const T t = P[j * ld + tid];
+            P[j * ld + tid] = P[p * ld + tid];
+            P[p * ld + tid] = t;
         }
         if (tid == 0) {
-            p_s = sidx[0];
-            ipiv[j] = sidx[0];
-            if (smax[0] == 0 && info[0] == 0) info[0] = j + 1;
+            ipiv[k0 + j] = k0 + p;
+            if (pb == T(0) && info[0] == 0) info[0] = k0 + j + 1;
         }
         __syncthreads();
-        const int p = p_s;
-        if (p != j) {
-            for (int c = tid; c < n; c += blockDim.x) {
-                const T t = A[(size_t)j * n + c];
-                A[(size_t)j * n + c] = A[(size_t)p * n + c];
-                A[(size_t)p * n + c] = t;
-            }
-        }
-        __syncthreads();
-        if (tid == 0) piv_s = A[(size_t)j * n + j];
-        __syncthreads();
-        const T piv = piv_s;
-        if (piv != 0) {
-            const T r = T(1) / piv;
-            for (int i = j + 1 + tid; i < n; i += blockDim.x) A[(size_t)i * n + j] *= r;
-        }
-        __syncthreads();
-        // rank-1 update inside the panel
-        const int w = kend - j - 1;
-        if (w > 0) {
-            for (int e = tid; e < (n - j - 1) * w; e += blockDim.x) {
-                const int i = j + 1 + e / w, c = j + 1 + e % w;
-                A[(size_t)i * n + c] -= A[(size_t)i * n + j] * A[(size_t)j * n + c];
+        const T piv = P[j * ld + j];
+        if (piv != T(0)) {
+            const T rcp = T(1) / piv;
+            for (int r = j + 1 + tid; r < m; r += kPanelThreads) {
+                const T l = P[r * ld + j] * rcp;
+                P[r * ld + j] = l;
+                for (int c = j + 1; c < nb; ++c) P[r * ld + c] -= l * P[j * ld + c];
             }
         }
         __syncthreads();
     }
+    for (int e = tid; e < m * nb; e += kPanelThreads) {
+        const int r = e / nb, c = e - r * nb;
+        A[(size_t)(k0 + r) * n + k0 + c] = P[r * ld + c];
+    }
 }
 
-// U12 = L11^{-1} A12 for the block row [k0, k0+nb), columns >= k0+nb
-template <typename T>
-__global__ void trsm_kernel(T* A, int n, int k0, int nb)
+// The panel's interchanges on every column outside it (dlaswp, in pivot
+// order), then U12 = L11^{-1} A12 on the columns right of it (unit lower
+// triangular L11).  One thread per column.  nb <= NB is the panel's width; a
+// panel narrower than NB (the last one of a matrix whose order is not a
+// multiple of NB) has no columns to its right.
+template <typename T, int NB>
+__global__ void __launch_bounds__(256) swap_trsm_kernel(T* A, int n, int k0, int nb, const int* ipiv)
 {
-    const int c = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
-    for (int r = 1; r < nb; ++r) {
-        T s = A[(size_t)(k0 + r) * n + c];
-        for (int l = 0; l < r; ++l) s -= A[(size_t)(k0 + r) * n + k0 + l] * A[(size_t)(k0 + l) * n + c];
-        A[(size_t)(k0 + r) * n + c] = s;
+    __shared__ T L[NB][NB + 1];
+    __shared__ int piv[NB];
+    const int tid = threadIdx.x;
+    for (int e = tid; e < nb * nb; e += 256) {
+        const int r = e / nb, c = e % nb;
+        L[r][c] = A[(size_t)(k0 + r) * n + k0 + c];
     }
+    if (tid < nb) piv[tid] = ipiv[k0 + tid];
+    __syncthreads();
+    const int c = blockIdx.x * 256 + tid;
+    const int cc = c < k0 ? c : c + nb;
+    if (cc >= n) return;
+#pragma unroll 1
+    for (int j = 0; j < nb; ++j) {
+        const int p = piv[j];
+        if (p != k0 + j) {
+            const T t = A[(size_t)(k0 + j) * n + cc];
+            A[(size_t)(k0 + j) * n + cc] = A[(size_t)p * n + cc];
+            A[(size_t)p * n + cc] = t;
+        }
+    }
+    if (cc < k0 + nb || nb != NB) return;
+    T u[NB];
+#pragma unroll
+    for (int r = 0; r < NB; ++r) u[r] = A[(size_t)(k0 + r) * n + cc];
+#pragma unroll
+    for (int l = 0; l < NB; ++l)
+#pragma unroll
+        for (int r = l + 1; r < NB; ++r) u[r] -= L[r][l] * u[l];
+#pragma unroll
+    for (int r = 1; r < NB; ++r) A[(size_t)(k0 + r) * n + cc] = u[r];
 }
 
-// A22 -= L21 U12, 64x64 tiles, 256 threads, 4x4 outputs per thread
+// A22 -= L21 U12 on the CUDA cores: 64 x 64 tiles, 256 threads, 4 x 4
+// outputs per thread.
 template <typename T>
 __global__ void __launch_bounds__(256) update_kernel(T* A, int n, int k0, int nb)
 {
-    __shared__ T Ls[64][kNB + 1];
-    __shared__ T Us[kNB][64 + 1];
+    __shared__ T Ls[64][kMaxNB + 1];
+    __shared__ T Us[kMaxNB][64 + 1];
     const int k1 = k0 + nb;
     const int r0 = k1 + blockIdx.y * 64, c0 = k1 + blockIdx.x * 64;
     const int tid = threadIdx.x;
@@ -149,56 +212,359 @@ __global__ void __launch_bounds__(256) update_kernel(T* A, int n, int k0, int nb
     }
 }
 
+// ------------------------------------------------------------------------
+// A22 -= L21 U12 in FP32 on the tensor cores (tcgen05.mma kind::tf32).
+//
+// One CTA of 128 threads per 128 x 128 output tile, K = NB (8, 16 or 32).
+// Operands are staged in shared memory in the canonical K-major layout
+// without swizzle: 8-row x 16-byte core matrices, the two 16-byte K halves of
+// one MMA (K = 8 TF32) LBO = 128 bytes apart, successive 8-row groups SBO =
+// 32 NB bytes apart.  Each FP32 operand x is split into hi = x with its 13 low
+// mantissa bits cleared (a TF32 value) and lo = x - hi (exact in FP32); the
+// accumulator in Tensor Memory receives hi*hi + hi*lo + lo*hi, which keeps the
+// product to about FP32 accuracy (the lo*lo term is below it).  One thread
+// issues the MMAs and commits them to an mbarrier; after a bounded wait every
+// warp reads its 32 lanes of the 128 x 128 FP32 accumulator (tcgen05.ld) and
+// subtracts them from A22.
+constexpr int kTcM = 128, kTcN = 128;
+constexpr uint32_t kTcCols = 128;            // TMEM columns allocated (N FP32 accumulators)
+constexpr long long kTcWaitLimit = 1 << 24;  // mbarrier polls before giving up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// UMMA shared-memory descriptor: start address, LBO and SBO in 16-byte units,
+// version 1 (Blackwell), no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3fff);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3fff) << 16;
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3fff) << 32;
+    d |= (uint64_t)1 << 46;  // version
+    return d;                // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor: F32 accumulator, TF32 A and B, both K-major, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc_tf32(int M, int N)
+{
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void tf32_split(float x, float& hi, float& lo)
+{
+    hi = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
+    lo = x - hi;
+}
+
+// byte offset of element (row, k) of a [rows][K] K-major operand
+__device__ __forceinline__ uint32_t kmajor_offset(int row, int k, int K)
+{
+    return (uint32_t)((row & 7) * 16 + (k >> 2) * 128 + (row >> 3) * 32 * K + (k & 3) * 4);
+}
+
+template <int NB>
+__global__ void __launch_bounds__(128) tc_update_kernel(float* A, int n, int k0, int* err)
+{
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    constexpr int OPB = kTcM * NB * 4;  // bytes of one operand tile
+    unsigned char* a_hi = tc_smem;
+    unsigned char* a_lo = a_hi + OPB;
+    unsigned char* b_hi = a_lo + OPB;
+    unsigned char* b_lo = b_hi + OPB;
+    __shared__ __align__(8) unsigned long long mbar;
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int k1 = k0 + NB;
+    const int r0 = k1 + blockIdx.y * kTcM, c0 = k1 + blockIdx.x * kTcN;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(kTcCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
+    }
+    // operands: A tile rows = L21 rows r0.., K = the panel columns; B tile
+    // rows = output columns c0.. (U12 transposed to K-major), K = panel rows
+    for (int e = tid; e < kTcM * NB; e += 128) {
+        const int row = e / NB, k = e % NB;
+        const float a = (r0 + row < n) ? A[(size_t)(r0 + row) * n + k0 + k] : 0.0f;
+        float hi, lo;
+        tf32_split(a, hi, lo);
+        const uint32_t off = kmajor_offset(row, k, NB);
+        *reinterpret_cast<float*>(a_hi + off) = hi;
+        *reinterpret_cast<float*>(a_lo + off) = lo;
+    }
+    for (int e = tid; e < kTcN * NB; e += 128) {
+        const int k = e / kTcN, col = e % kTcN;  // consecutive threads: consecutive columns of a U12 row
+        const float b = (c0 + col < n) ? A[(size_t)(k0 + k) * n + c0 + col] : 0.0f;
+        float hi, lo;
+        tf32_split(b, hi, lo);
+        const uint32_t off = kmajor_offset(col, k, NB);
+        *reinterpret_cast<float*>(b_hi + off) = hi;
+        *reinterpret_cast<float*>(b_lo + off) = lo;
+    }
+    // generic-proxy shared-memory writes -> visible to the tensor cores
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+
+    if (tid == 0) {
+        constexpr uint32_t idesc = umma_idesc_tf32(kTcM, kTcN);
+        const uint32_t lbo = 128, sbo = 32 * NB;
+        const uint32_t sa_hi = smem_u32(a_hi), sa_lo = smem_u32(a_lo);
+        const uint32_t sb_hi = smem_u32(b_hi), sb_lo = smem_u32(b_lo);
+        uint32_t acc = 0;
+#pragma unroll
+        for (int ks = 0; ks < NB / 8; ++ks) {
+            const uint32_t koff = ks * 256;  // K = 8 TF32 = two 16-byte chunks, 128 bytes apart
+            const uint64_t ah = umma_desc(sa_hi + koff, lbo, sbo), al = umma_desc(sa_lo + koff, lbo, sbo);
+            const uint64_t bh = umma_desc(sb_hi + koff, lbo, sbo), bl = umma_desc(sb_lo + koff, lbo, sbo);
+            const uint64_t pairs[3][2] = {{ah, bh}, {ah, bl}, {al, bh}};
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(pairs[q][0]), "l"(pairs[q][1]), "r"(idesc), "r"(acc));
+                acc = 1;
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&mbar))
+                     : "memory");
+    }
+    // bounded wait for the MMAs (phase 0)
+    bool done = false;
+    for (long long it = 0; it < kTcWaitLimit && !done; ++it) {
+        uint32_t ok = 0;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(ok)
+            : "r"(smem_u32(&mbar)), "r"(0)
+            : "memory");
+        done = ok != 0;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!done) {
+        if (tid == 0) atomicExch(err, 1);
+    } else {
+        // this warp's 32 lanes = rows 32 warp + lane of the tile
+        const int row = r0 + 32 * warp + lane;
+#pragma unroll 1
+        for (int cb = 0; cb < kTcN; cb += 32) {
+            uint32_t v[32];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)cb;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < n) {
+                float* crow = A + (size_t)row * n + c0 + cb;
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    if (c0 + cb + j < n) crow[j] -= __uint_as_float(v[j]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols));
+    }
+}
+
+// 1 (default): the FP32 trailing updates run on the tensor cores; 0
+// ($PCC_LU_TC=0): on the CUDA cores (the same kernel as FP64), for comparison.
+bool lu_tensor_cores()
+{
+    const char* v = std::getenv("PCC_LU_TC");
+    return !(v && std::string(v) == "0");
+}
+
 template <typename T>
-cudaError_t lu_factor(T* A, int n, int* ipiv, int* info, cudaStream_t st)
+cudaError_t launch_swap_trsm(T* A, int n, int k0, int nb, int nb_max, const int* ipiv, cudaStream_t st)
+{
+    const int cols = n - nb;
+    if (cols <= 0) return cudaSuccess;
+    const int grid = (cols + 255) / 256;
+    switch (nb_max) {
+        case 32: swap_trsm_kernel<T, 32><<<grid, 256, 0, st>>>(A, n, k0, nb, ipiv); break;
+        case 16: swap_trsm_kernel<T, 16><<<grid, 256, 0, st>>>(A, n, k0, nb, ipiv); break;
+        case 8: swap_trsm_kernel<T, 8><<<grid, 256, 0, st>>>(A, n, k0, nb, ipiv); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tc_update(float* A, int n, int k0, int nb, int* err, cudaStream_t st)
+{
+    const int rest = n - k0 - nb;
+    dim3 g((rest + kTcN - 1) / kTcN, (rest + kTcM - 1) / kTcM);
+    const size_t smem = 4 * (size_t)kTcM * nb * sizeof(float);
+    cudaError_t e = cudaSuccess;
+    switch (nb) {
+        case 32:
+            e = cudaFuncSetAttribute(tc_update_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e == cudaSuccess) tc_update_kernel<32><<<g, 128, smem, st>>>(A, n, k0, err);
+            break;
+        case 16:
+            e = cudaFuncSetAttribute(tc_update_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e == cudaSuccess) tc_update_kernel<16><<<g, 128, smem, st>>>(A, n, k0, err);
+            break;
+        case 8:
+            e = cudaFuncSetAttribute(tc_update_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e == cudaSuccess) tc_update_kernel<8><<<g, 128, smem, st>>>(A, n, k0, err);
+            break;
+        default: return cudaErrorInvalidValue;
+    }
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+// info[0]: 1-based index of the first zero pivot (0: none); info[2]: the
+// tensor-core update gave up waiting (then the factors are not used).
+template <typename T>
+cudaError_t lu_factor(T* A, int n, int* ipiv, int* info, bool tc, cudaStream_t st)
 {
     cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    for (int k0 = 0; k0 < n; k0 += kNB) {
-        const int nb = min(kNB, n - k0);
-        panel_kernel<T><<<1, 256, 0, st>>>(A, n, k0, nb, ipiv, info);
+    const int nb_max = panel_nb(n, sizeof(T));
+    const size_t psmem_max = (size_t)n * (nb_max + 1) * sizeof(T);
+    if (psmem_max > kPanelSmemCap) return cudaErrorInvalidValue;  // n above lu_max_order()
+    e = cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem_max);
+    if (e != cudaSuccess) return e;
+    for (int k0 = 0; k0 < n; k0 += nb_max) {
+        const int nb = n - k0 < nb_max ? n - k0 : nb_max;
+        const size_t psmem = (size_t)(n - k0) * (nb + 1) * sizeof(T);
+        panel_kernel<T><<<1, kPanelThreads, psmem, st>>>(A, n, k0, nb, ipiv, info);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = launch_swap_trsm<T>(A, n, k0, nb, nb_max, ipiv, st)) != cudaSuccess) return e;
         const int rest = n - k0 - nb;
         if (rest > 0) {
-            trsm_kernel<T><<<(rest + 127) / 128, 128, 0, st>>>(A, n, k0, nb);
+            if constexpr (sizeof(T) == 4) {
+                if (tc) {
+                    if ((e = launch_tc_update(reinterpret_cast<float*>(A), n, k0, nb, info + 2, st)) != cudaSuccess)
+                        return e;
+                    continue;
+                }
+            }
             dim3 g((rest + 63) / 64, (rest + 63) / 64);
             update_kernel<T><<<g, 256, 0, st>>>(A, n, k0, nb);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
 
 // x = A^{-1} b from the factors (dgetrs): row swaps, unit-lower forward and
-// upper backward substitution.  One CTA; TB is the type of the vectors.
+// upper backward substitution in blocks of 32.  One CTA of 512 threads; x
+// lives in shared memory (n TB values).  skip: optional device flag; a
+// nonzero value makes the call return at once (the refinement loop's "done").
+constexpr int kGetrsThreads = 512;
+
 template <typename T, typename TB>
-__global__ void __launch_bounds__(1024) lu_apply_kernel(const T* A, int n, const int* ipiv, const TB* b, TB* x)
+__global__ void __launch_bounds__(kGetrsThreads) getrs_kernel(const T* A, int n, const int* ipiv, const TB* b, TB* x,
+                                                              const int* skip)
 {
-    const int tid = threadIdx.x;
-    if (tid == 0)
-        for (int i = 0; i < n; ++i) x[i] = b[i];
+    if (skip && *(const volatile int*)skip) return;
+    extern __shared__ __align__(16) unsigned char getrs_smem[];
+    TB* xs = reinterpret_cast<TB*>(getrs_smem);
+    constexpr int NT = kGetrsThreads, NWS = NT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < n; i += NT) xs[i] = b[i];
     __syncthreads();
     if (tid == 0)
         for (int i = 0; i < n; ++i) {
             const int p = ipiv[i];
             if (p != i) {
-                const TB t = x[i];
-                x[i] = x[p];
-                x[p] = t;
+                const TB t = xs[i];
+                xs[i] = xs[p];
+                xs[p] = t;
             }
         }
     __syncthreads();
-    for (int j = 0; j < n; ++j) {
-        const TB yj = x[j];
-        for (int i = j + 1 + tid; i < n; i += blockDim.x) x[i] -= (TB)A[(size_t)i * n + j] * yj;
+    // forward: L y = P b, L unit lower
+    for (int jb = 0; jb < n; jb += 32) {
+        const int bw = n - jb < 32 ? n - jb : 32;
+        if (warp == 0) {
+            TB xv = lane < bw ? xs[jb + lane] : TB(0);
+            T row[32];
+#pragma unroll
+            for (int l = 0; l < 32; ++l)
+                row[l] = (lane < bw && l < lane) ? A[(size_t)(jb + lane) * n + jb + l] : T(0);
+#pragma unroll
+            for (int l = 0; l < 32; ++l) {
+                const TB xl = __shfl_sync(0xffffffffu, xv, l);
+                if (l < bw && lane > l) xv -= (TB)row[l] * xl;
+            }
+            if (lane < bw) xs[jb + lane] = xv;
+        }
+        __syncthreads();
+        for (int i = jb + bw + warp; i < n; i += NWS) {
+            TB s = lane < bw ? (TB)A[(size_t)i * n + jb + lane] * xs[jb + lane] : TB(0);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) xs[i] -= s;
+        }
         __syncthreads();
     }
-    for (int j = n - 1; j >= 0; --j) {
-        if (tid == 0) x[j] = x[j] / (TB)A[(size_t)j * n + j];
+    // backward: U x = y
+    for (int je = n; je > 0; je -= 32) {
+        const int jb = je - 32 > 0 ? je - 32 : 0, bw = je - jb;
+        if (warp == 0) {
+            TB xv = lane < bw ? xs[jb + lane] : TB(0);
+            T row[32];
+#pragma unroll
+            for (int l = 0; l < 32; ++l)
+                row[l] = (lane < bw && l >= lane && l < bw) ? A[(size_t)(jb + lane) * n + jb + l] : T(1);
+#pragma unroll
+            for (int l = 31; l >= 0; --l) {
+                if (l < bw && lane == l) xv = xv / (TB)row[l];
+                const TB xl = __shfl_sync(0xffffffffu, xv, l);
+                if (l < bw && lane < l) xv -= (TB)row[l] * xl;
+            }
+            if (lane < bw) xs[jb + lane] = xv;
+        }
         __syncthreads();
-        const TB yj = x[j];
-        for (int i = tid; i < j; i += blockDim.x) x[i] -= (TB)A[(size_t)i * n + j] * yj;
+        for (int i = warp; i < jb; i += NWS) {
+            TB s = lane < bw ? (TB)A[(size_t)i * n + jb + lane] * xs[jb + lane] : TB(0);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) xs[i] -= s;
+        }
         __syncthreads();
     }
+    for (int i = tid; i < n; i += NT) x[i] = xs[i];
+}
+
+template <typename T, typename TB>
+cudaError_t launch_getrs(const T* A, int n, const int* ipiv, const TB* b, TB* x, const int* skip, cudaStream_t st)
+{
+    const size_t smem = (size_t)n * sizeof(TB);
+    if (smem > 48 * 1024) {
+        cudaError_t e =
+            cudaFuncSetAttribute(getrs_kernel<T, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    getrs_kernel<T, TB><<<1, kGetrsThreads, smem, st>>>(A, n, ipiv, b, x, skip);
+    return cudaGetLastError();
 }
 
 __global__ void to_float_kernel(const double* a, float* b, size_t cnt)
@@ -207,36 +573,63 @@ __global__ void to_float_kernel(const double* a, float* b, size_t cnt)
         b[i] = (float)a[i];
 }
 
-// r = b - A x (FP64), one warp per row; out[0] = ||r||_inf, out[1] = ||x||_inf
-__global__ void residual_kernel(const double* A, const double* b, const double* x, double* r, int n,
-                                unsigned long long* norms)
+// State of the refinement loop on the device.
+struct IrState {
+    unsigned long long norms[3];  // ||r||_inf, ||x||_inf, ||A||_inf (bit patterns, for atomicMax)
+    int done;                     // 1 converged, 2 stopped (non-finite residual), 0 running
+    int steps;                    // sweeps taken before convergence
+    double resid;                 // ||r|| / (||A|| ||x||) of the last check
+};
+
+// r = b - A x (FP64), one warp per row, and the two vector norms
+__global__ void residual_kernel(const double* A, const double* b, const double* x, double* r, int n, IrState* s)
 {
+    if (s->done) return;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x & 31;
     if (warp >= n) return;
-    double s = 0.0;
-    for (int j = lane; j < n; j += 32) s = fma(A[(size_t)warp * n + j], x[j], s);
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    double acc = 0.0;
+    for (int j = lane; j < n; j += 32) acc = fma(A[(size_t)warp * n + j], x[j], acc);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) {
-        const double ri = b[warp] - s;
+        const double ri = b[warp] - acc;
         r[warp] = ri;
-        atomicMax(&norms[0], __double_as_longlong(fabs(ri)));
-        atomicMax(&norms[1], __double_as_longlong(fabs(x[warp])));
+        atomicMax(&s->norms[0], __double_as_longlong(fabs(ri)));
+        atomicMax(&s->norms[1], __double_as_longlong(fabs(x[warp])));
     }
 }
 
+// dsgesv's test after sweep `step`: converged when ||r|| <= sqrt(n) eps ||A|| ||x||
+__global__ void ir_check_kernel(IrState* s, int n, int step)
+{
+    if (s->done) return;
+    const double rn = __longlong_as_double(s->norms[0]), xn = __longlong_as_double(s->norms[1]);
+    const double an = __longlong_as_double(s->norms[2]);
+    const double eps = 1.1102230246251565e-16;  // dlamch('Epsilon')
+    s->resid = (an > 0 && xn > 0) ? rn / (an * xn) : rn;
+    s->steps = step;
+    if (!isfinite(s->resid)) {
+        s->done = 2;
+    } else if (rn <= sqrt((double)n) * eps * an * xn) {
+        s->done = 1;
+    }
+    s->norms[0] = 0;
+    s->norms[1] = 0;
+}
+
 // ||A||_inf
-__global__ void rownorm_kernel(const double* A, int n, unsigned long long* out)
+__global__ void rownorm_kernel(const double* A, int n, IrState* s)
 {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x & 31;
     if (warp >= n) return;
-    double s = 0.0;
-    for (int j = lane; j < n; j += 32) s += fabs(A[(size_t)warp * n + j]);
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) atomicMax(out, __double_as_longlong(s));
+    double acc = 0.0;
+    for (int j = lane; j < n; j += 32) acc += fabs(A[(size_t)warp * n + j]);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) atomicMax(&s->norms[2], __double_as_longlong(acc));
 }
 
-__global__ void axpy_kernel(double* x, const double* d, int n)
+__global__ void axpy_kernel(double* x, const double* d, int n, const IrState* s)
 {
+    if (s->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x[i] += d[i];
 }
@@ -261,10 +654,12 @@ __global__ void fma_probe_kernel(double* out, int iters, double seed)
 
 }  // namespace
 
+int lu_max_order() { return (int)(kPanelSmemCap / (9 * sizeof(double))); }
+
 size_t lu_mixed_work_bytes(int n)
 {
-    // float copy of A, r and d vectors (double), norms
-    return (size_t)n * n * sizeof(float) + 4 * (size_t)n * sizeof(double) + 64;
+    // float copy of A, r and d vectors (double), the refinement state
+    return (size_t)n * n * sizeof(float) + 4 * (size_t)n * sizeof(double) + sizeof(IrState) + 64;
 }
 
 cudaError_t lu_solve_fp64(const double* dA, const double* db, double* dx, int n, double* work, int* ipiv, int* info,
@@ -272,13 +667,9 @@ cudaError_t lu_solve_fp64(const double* dA, const double* db, double* dx, int n,
 {
     (void)work;
     double* A = const_cast<double*>(dA);  // factorised in place (the caller's working copy)
-    cudaError_t e = lu_factor<double>(A, n, ipiv, info, st);
+    cudaError_t e = lu_factor<double>(A, n, ipiv, info, false, st);
     if (e != cudaSuccess) return e;
-    lu_apply_kernel<double, double><<<1, 1024, 0, st>>>(A, n, ipiv, db, dx);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    int zero = 0;
-    (void)zero;
+    if ((e = launch_getrs<double, double>(A, n, ipiv, db, dx, nullptr, st)) != cudaSuccess) return e;
     return cudaMemsetAsync(info + 1, 0, sizeof(int), st);  // no host source: capturable
 }
 
@@ -291,55 +682,52 @@ cudaError_t lu_solve_mixed(const double* dA, const double* db, double* dx, int n
     float* A32 = static_cast<float*>(work);
     double* r = reinterpret_cast<double*>(A32 + (size_t)n * n);
     double* d = r + n;
-    unsigned long long* norms = reinterpret_cast<unsigned long long*>(d + 2 * n);
+    IrState* s = reinterpret_cast<IrState*>(d + 2 * n);
     cudaError_t e;
     const size_t nn = (size_t)n * n;
+    const bool tc = lu_tensor_cores();
+    if ((e = cudaMemsetAsync(info + 2, 0, sizeof(int), st)) != cudaSuccess) return e;
     to_float_kernel<<<1024, 256, 0, st>>>(dA, A32, nn);
-    if ((e = lu_factor<float>(A32, n, ipiv, info, st)) != cudaSuccess) return e;
-    // ||A||_inf
-    if ((e = cudaMemsetAsync(norms, 0, 3 * sizeof(unsigned long long), st)) != cudaSuccess) return e;
-    rownorm_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(dA, n, norms + 2);
+    if ((e = lu_factor<float>(A32, n, ipiv, info, tc, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(s, 0, sizeof(IrState), st)) != cudaSuccess) return e;
+    rownorm_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(dA, n, s);
     // x0 = LU32 \ b (computed in FP64 on the FP32 factors)
-    lu_apply_kernel<float, double><<<1, 1024, 0, st>>>(A32, n, ipiv, db, dx);
-    unsigned long long h[3];
-    int hinfo = 0;
-    if ((e = cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-    const double eps = 1.1102230246251565e-16;  // dlamch('Epsilon')
-    int steps = 0, fallback = (hinfo != 0) ? 1 : 0;
-    double resid = -1.0;
-    bool ok = false;
-    for (; !fallback && steps <= max_refine; ++steps) {
-        if ((e = cudaMemsetAsync(norms, 0, 2 * sizeof(unsigned long long), st)) != cudaSuccess) return e;
-        residual_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(dA, db, dx, r, n, norms);
-        if ((e = cudaMemcpyAsync(h, norms, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-            return e;
-        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-        double rn, xn, an;
-        std::memcpy(&rn, &h[0], 8);
-        std::memcpy(&xn, &h[1], 8);
-        std::memcpy(&an, &h[2], 8);
-        resid = (an > 0 && xn > 0) ? rn / (an * xn) : rn;
-        if (!std::isfinite(resid)) break;
-        if (rn <= std::sqrt((double)n) * eps * an * xn) {
-            ok = true;
-            break;
+    if ((e = launch_getrs<float, double>(A32, n, ipiv, db, dx, nullptr, st)) != cudaSuccess) return e;
+    // Refinement sweeps in chunks: each sweep checks the previous iterate
+    // (residual + dsgesv test) and, unless the test passed, adds the correction
+    // LU32 \ r.  The host looks at the state once per chunk.
+    IrState hs{};
+    int hinfo[3] = {0, 0, 0};
+    int next = 0;
+    const int chunk = 3;
+    for (;;) {
+        const int upto = next + chunk - 1 < max_refine ? next + chunk - 1 : max_refine;
+        for (int step = next; step <= upto; ++step) {
+            residual_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(dA, db, dx, r, n, s);
+            ir_check_kernel<<<1, 1, 0, st>>>(s, n, step);
+            if (step == max_refine) break;  // the last check takes no correction
+            if ((e = launch_getrs<float, double>(A32, n, ipiv, r, d, &s->done, st)) != cudaSuccess) return e;
+            axpy_kernel<<<(n + 255) / 256, 256, 0, st>>>(dx, d, n, s);
         }
-        if (steps == max_refine) break;
-        lu_apply_kernel<float, double><<<1, 1024, 0, st>>>(A32, n, ipiv, r, d);
-        axpy_kernel<<<(n + 255) / 256, 256, 0, st>>>(dx, d, n);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(&hs, s, sizeof(IrState), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(hinfo, info, 3 * sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+        next = upto + 1;
+        if (hs.done || hinfo[0] != 0 || hinfo[2] != 0 || next > max_refine) break;
     }
-    if (steps_out) *steps_out = steps;
-    if (resid_out) *resid_out = resid;
+    const bool ok = hs.done == 1 && hinfo[0] == 0 && hinfo[2] == 0;
+    if (steps_out) *steps_out = hs.steps;
+    if (resid_out) *resid_out = hs.resid;
+    int fallback = 0;
     if (!ok) {
         // LAPACK dsgesv falls back to dgetrf/dgetrs in double precision
         double* A = const_cast<double*>(dA);
-        if ((e = lu_factor<double>(A, n, ipiv, info, st)) != cudaSuccess) return e;
-        lu_apply_kernel<double, double><<<1, 1024, 0, st>>>(A, n, ipiv, db, dx);
+        if ((e = lu_factor<double>(A, n, ipiv, info, false, st)) != cudaSuccess) return e;
+        if ((e = launch_getrs<double, double>(A, n, ipiv, db, dx, nullptr, st)) != cudaSuccess) return e;
         fallback = 1;
     } else {
-        int zero = 0;
-        if ((e = cudaMemcpyAsync(info, &zero, sizeof(int), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(info, 0, sizeof(int), st)) != cudaSuccess) return e;
     }
     if ((e = cudaMemcpyAsync(info + 1, &fallback, sizeof(int), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
     return cudaStreamSynchronize(st);

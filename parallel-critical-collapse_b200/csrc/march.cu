@@ -4,6 +4,7 @@
 // PCC_MARCH_DISPATCH, the launcher that selects among them and the autotuner
 // that picks the schedule per (device, Ntau, stages).
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -15,7 +16,7 @@ namespace pcc {
 
 namespace {
 
-template <int N, int S, bool PAIR>
+template <int N, int S, int PAIR>
 constexpr int min_blocks()
 {
     // The radix-8 RHS needs ~230 registers per thread without spilling, so a
@@ -24,7 +25,7 @@ constexpr int min_blocks()
     return nt <= 128 ? 2 : 1;
 }
 
-template <int N, int S, bool PAIR>
+template <int N, int S, int PAIR>
 cudaError_t launch_shape(const MarchParams& P, int max_ctas, cudaStream_t st, MarchLaunchInfo* info)
 {
     using K = MarchShape<N, S, PAIR>;
@@ -52,7 +53,7 @@ cudaError_t launch_shape(const MarchParams& P, int max_ctas, cudaStream_t st, Ma
     return cudaGetLastError();
 }
 
-template <int N, bool PAIR>
+template <int N, int PAIR>
 cudaError_t launch_n(int stages, const MarchParams& P, int max_ctas, cudaStream_t st, MarchLaunchInfo* info)
 {
     switch (stages) {
@@ -73,7 +74,7 @@ cudaError_t PCC_CAT4(launch_march_n, PCC_MARCH_N, _p, PCC_MARCH_PAIR)(int stages
                                                                      int max_ctas, cudaStream_t st,
                                                                      MarchLaunchInfo* info)
 {
-    return launch_n<PCC_MARCH_N, PCC_MARCH_PAIR != 0>(stages, P, max_ctas, st, info);
+    return launch_n<PCC_MARCH_N, PCC_MARCH_PAIR>(stages, P, max_ctas, st, info);
 }
 #endif
 
@@ -118,6 +119,7 @@ PCC_DECL(512)
 PCC_DECL(1024)
 PCC_DECL(2048)
 #undef PCC_DECL
+cudaError_t launch_march_n1024_p2(int, const MarchParams&, int, cudaStream_t, MarchLaunchInfo*);
 
 bool march_supported(int ntau, int stages)
 {
@@ -127,13 +129,21 @@ bool march_supported(int ntau, int stages)
 
 namespace {
 
-// Autotuned transform schedule per (device, Ntau, stages): 1 paired, 0 single.
+// Autotuned transform schedule per (device, Ntau, stages): 0 single, 1
+// paired, 2 paired with the warp-exchange transforms (Ntau 1024, 2 stages).
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int>, MarchTuning> g_tuned;
 
-cudaError_t launch_variant(int ntau, int stages, const MarchParams& P, int max_ctas, cudaStream_t st,
-                           MarchLaunchInfo* info, bool pair)
+bool schedule_available(int ntau, int stages, int sched)
 {
+    return sched == 0 || sched == 1 || (sched == 2 && ntau == 1024 && stages == 2);
+}
+
+cudaError_t launch_variant(int ntau, int stages, const MarchParams& P, int max_ctas, cudaStream_t st,
+                           MarchLaunchInfo* info, int sched)
+{
+    if (sched == 2 && schedule_available(ntau, stages, 2)) return launch_march_n1024_p2(stages, P, max_ctas, st, info);
+    const bool pair = sched != 0;
 #define PCC_CASE(n)                                                                                           \
     case n:                                                                                                   \
         return pair ? launch_march_n##n##_p1(stages, P, max_ctas, st, info)                                   \
@@ -173,17 +183,23 @@ cudaError_t launch_march(int ntau, int stages, const MarchParams& P, int max_cta
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     MarchTuning t{};
-    const bool pair = march_tuning(dev, ntau, stages, &t) ? t.pair != 0 : true;  // untuned: paired
-    return launch_variant(ntau, stages, P, max_ctas, st, info, pair);
+    int sched = march_tuning(dev, ntau, stages, &t) ? t.pair : 1;  // untuned: paired
+    if (const char* f = std::getenv("PCC_MARCH_SCHEDULE")) {
+        // a fixed schedule for every shape that has it (0, 1 or 2)
+        const int v = std::atoi(f);
+        if (schedule_available(ntau, stages, v)) sched = v;
+    }
+    return launch_variant(ntau, stages, P, max_ctas, st, info, sched);
 }
 
-// Times both transform schedules on the kernel's single-RHS mode: items
-// marching no step, one RHS evaluation each, over sixteen waves of sweep
-// slots (about half a millisecond at Ntau = 1024), from a smooth synthetic
-// state (Delta = 3.4 in its slot), best of five.  The paired schedule is kept
-// unless the single one is more than 3 % faster: on a full march the two
-// differ by a few per cent, less than a short probe's noise.  The choice is
-// recorded for (device, Ntau, stages).  Allocates and frees its own buffers.
+// Times the transform schedules of the shape on the kernel's single-RHS mode:
+// items marching no step, one RHS evaluation each, over sixteen waves of
+// sweep slots (about half a millisecond at Ntau = 1024), from a smooth
+// synthetic state (Delta = 3.4 in its slot), best of five.  The paired
+// schedule is kept unless another one is more than 3 % faster: on a full
+// march the schedules differ by a few per cent, less than a short probe's
+// noise.  The choice is recorded for (device, Ntau, stages).  Allocates and
+// frees its own buffers.
 cudaError_t march_autotune(int ntau, int stages, const double2* tw, cudaStream_t st, MarchTuning* out)
 {
     int dev = 0, sms = 0;
@@ -209,8 +225,9 @@ cudaError_t march_autotune(int ntau, int stages, const double2* tw, cudaStream_t
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_x, xs.data(), items * sizeof(double), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaEventCreate(&a);
     if (e == cudaSuccess) e = cudaEventCreate(&b);
-    double ms[2] = {0.0, 0.0};
-    for (int v = 0; v < 2 && e == cudaSuccess; ++v) {
+    double ms[3] = {0.0, 0.0, 0.0};
+    for (int v = 0; v < 3 && e == cudaSuccess; ++v) {
+        if (!schedule_available(ntau, stages, v)) continue;
         MarchParams P{};
         P.n_items = items;
         P.mode = 1;
@@ -228,7 +245,7 @@ cudaError_t march_autotune(int ntau, int stages, const double2* tw, cudaStream_t
         for (int rep = 0; rep < 6 && e == cudaSuccess; ++rep) {  // one warm-up, best of five
             e = cudaMemsetAsync(d_cnt, 0, sizeof(int), st);
             if (e == cudaSuccess) e = cudaEventRecord(a, st);
-            if (e == cudaSuccess) e = launch_variant(ntau, stages, P, 0, st, nullptr, v == 1);
+            if (e == cudaSuccess) e = launch_variant(ntau, stages, P, 0, st, nullptr, v);
             if (e == cudaSuccess) e = cudaEventRecord(b, st);
             if (e == cudaSuccess) e = cudaEventSynchronize(b);
             float t = 0.0f;
@@ -245,9 +262,16 @@ cudaError_t march_autotune(int ntau, int stages, const double2* tw, cudaStream_t
     cudaFree(d_cnt);
     if (e != cudaSuccess) return e;
     MarchTuning t{};
-    t.pair = ms[0] < 0.97 * ms[1] ? 0 : 1;
+    t.pair = 1;
+    double best = 0.97 * ms[1];
+    for (int v : {0, 2})
+        if (ms[v] > 0.0 && ms[v] < best) {
+            best = ms[v];
+            t.pair = v;
+        }
     t.ms_single = ms[0];
     t.ms_pair = ms[1];
+    t.ms_wx = ms[2];
     march_set_tuning(dev, ntau, stages, t);
     if (out) *out = t;
     return cudaSuccess;

@@ -69,7 +69,10 @@ struct MarchParams {
     double* snap;                  // [slot][N] states at the start of the steps snap_slot marks
 };
 
-template <int N, int S, bool PAIR = true>
+// Transform schedules: 0 single transforms, 1 paired (dft_m2), 2 paired with
+// the warp-exchange length-512 transforms (Ntau = 1024 only; other sizes
+// treat 2 as 1).
+template <int N, int S, int PAIR = 1>
 struct MarchShape {
     static constexpr int M = N / 2;
     static constexpr int Q = N / 4;
@@ -89,7 +92,8 @@ struct MarchShape {
     // paired transforms (dft_m2) need a second set of exchange pairs; shapes
     // whose shared memory would not fit keep single transforms, and PAIR =
     // false (a variant the autotuner may pick) never pairs
-    static constexpr bool DUAL = PAIR && (size_t)SPC * (2 * EXA + YS + YK + UV + MISC) * 16 <= 200 * 1024;
+    static constexpr bool DUAL = PAIR != 0 && (size_t)SPC * (2 * EXA + YS + YK + UV + MISC) * 16 <= 200 * 1024;
+    static constexpr bool WX = PAIR == 2 && DUAL && M == 512 && S * TG == STP;  // warp-exchange transforms
     static constexpr int EX = DUAL ? 2 * EXA : EXA;           // exchange double2s
     static constexpr int PER_SWEEP = EX + YS + YK + UV + MISC; // double2 per sweep
     static constexpr size_t SMEM = (size_t)SPC * PER_SWEEP * sizeof(double2);
@@ -166,8 +170,18 @@ __host__ __device__ constexpr int pass_table_offset(int M, int NS)
     for (int s = 8; s < NS; s *= 8) off += (pass_radix(M, s) - 1) * s;
     return off;
 }
+// Tables of the warp-exchange length-512 transforms (Ntau = 1024, below),
+// after the pass tables: T64[k][q] = exp(+2 pi i q k/64) (k, q < 8), then
+// TB_ST[r][t] = exp(+2 pi i (t&7)((t>>3) + 8r)/512) and TB_TS[r][t] =
+// exp(+2 pi i (t>>3)((t&7) + 8r)/512) for r < 8, t < 64; every entry is a copy
+// of a point twiddle.
+__host__ __device__ constexpr int w512_table_offset(int N) { return N + pass_table_offset(N / 2, N / 2); }
+constexpr int kW512Tables = 64 + 512 + 512;
 // double2 entries of the twiddle buffer of a march over Ntau = N
-__host__ __device__ constexpr int march_twiddle_count(int N) { return N + pass_table_offset(N / 2, N / 2); }
+__host__ __device__ constexpr int march_twiddle_count(int N)
+{
+    return w512_table_offset(N) + (N == 1024 ? kW512Tables : 0);
+}
 
 // Twiddles of one Stockham pass (radix R, span NS) for thread t: element r of
 // butterfly u = t + TG u' is multiplied by w_M^{SG r k M/(NS R)}, k = j mod NS.
@@ -232,6 +246,15 @@ __device__ __forceinline__ void fetch_point_twiddles(double2* pj, int t, const d
 {
 #pragma unroll
     for (int q = 0; q < 8; ++q) pj[q] = __ldg(&twN[t + TG * q + zoff]);
+}
+
+// the per-point twiddles w_N^j (N = 1024) in layout T of the warp-exchange
+// transforms: register q of thread t holds point j = (t >> 3) + 8 (t & 7) + 64 q
+__device__ __forceinline__ void fetch_point_twiddles_t(double2* pj, int t, const double2* __restrict__ twN, int zoff)
+{
+    const int j0 = (t >> 3) + 8 * (t & 7);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) pj[q] = __ldg(&twN[j0 + 64 * q + zoff]);
 }
 
 template <int TG>
@@ -371,6 +394,178 @@ __device__ __forceinline__ void dft_m2(double2 (&v)[8], double2 (&u)[8], double2
     }
 }
 
+// ------------------------------------------- warp-exchange length-512 DFT
+// A length-512 transform on a stage group of 64 threads (two warps) in which
+// one of the two data exchanges stays inside a warp.  Index p = a + 8b + 64c
+// (digits < 8), k = ka + 8kb + 64kc:
+//   X[k] = sum_a w^{a(ka+8kb)} w8^{a kc} sum_b w64^{b ka} w8^{b kb} sum_c w8^{c ka} x[p]
+// with w = exp(SG 2 pi i/512): a radix-8 pass over each digit, registers
+// holding the digit being summed.  A thread t has lo = t & 7, hi = t >> 3
+// (hi's top bit is the warp), and its register q holds index
+//   layout S:  lo + 8 hi + 64 q      layout T:  hi + 8 lo + 64 q.
+// An exchange swaps the register digit with one thread digit: with lo (the
+// thread keeps hi) it stays inside a warp and needs only __syncwarp; with hi
+// it crosses warps and needs the group barrier.  A transform from S sums c,
+// then b (= hi: cross-warp exchange), then a (= lo: warp-local) and leaves
+// its output in layout T; a transform from T sums c, b (= lo: warp-local),
+// a (= hi: cross-warp) and leaves layout S.  The RHS alternates them: the
+// state and spectra live in layout S, the physical-space fields in layout T.
+//
+// Buffers (b0, b1 of the stage).  Every read is "thread t, register q reads
+// t + 64 q", so a warp reads only the entries whose bits 3..5 are its own hi
+// values; a warp-local exchange writes only such entries too.  An S->T
+// transform exchanges through b0 twice (the warp-local exchange rewrites the
+// warp's own part of b0 after the warp has read it); a T->S transform makes
+// its warp-local exchange in b0 and its cross-warp one in b1; the stage RHS
+// then goes to b1 (each thread its own slots).  Between two writes of a
+// buffer by different warps there is always a group barrier after the last
+// read of the first write, since the two kinds of transform alternate.
+// The index swizzle i ^ ((i >> 6) & 7) makes every write and read pattern
+// map the 8 lanes of a 16-byte access phase to 8 distinct bank groups.
+__device__ __forceinline__ int swz64(int i) { return i ^ ((i >> 6) & 7); }
+
+// exchange write patterns: register r of thread t goes to
+//   cross: thread lo + 8 r, register hi      (index lo + 8 r + 64 hi)
+//   local: thread r + 8 hi, register lo      (index r + 8 hi + 64 lo)
+__device__ __forceinline__ int wx_cross(int t, int r) { return swz64((t & 7) + 8 * r + 64 * (t >> 3)); }
+__device__ __forceinline__ int wx_local(int t, int r) { return swz64(r + 8 * (t >> 3) + 64 * (t & 7)); }
+
+template <int SG, bool IN_T>
+__device__ __forceinline__ void w512_fetch_a(double2 (&w)[7], int t, const double2* __restrict__ tab, int zoff)
+{
+    // after the first exchange: register q holds digit b, twiddle w64^{b ka},
+    // ka = t >> 3 (from S) or t & 7 (from T)
+    const int k = IN_T ? (t & 7) : (t >> 3);
+#pragma unroll
+    for (int q = 1; q < 8; ++q) {
+        double2 x = __ldg(&tab[k * 8 + q + zoff]);
+        if (SG < 0) x.y = -x.y;
+        w[q - 1] = x;
+    }
+}
+
+template <int SG, bool IN_T>
+__device__ __forceinline__ void w512_fetch_b(double2 (&w)[8], int t, const double2* __restrict__ tab, int zoff)
+{
+    const double2* __restrict__ tb = tab + 64 + (IN_T ? 512 : 0);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        double2 x = __ldg(&tb[r * 64 + t + zoff]);
+        if (SG < 0) x.y = -x.y;
+        w[r] = x;
+    }
+}
+
+__device__ __forceinline__ void w512_store(const double2 (&v)[8], double2* __restrict__ buf, int t, bool cross)
+{
+#pragma unroll
+    for (int r = 0; r < 8; ++r) buf[cross ? wx_cross(t, r) : wx_local(t, r)] = v[r];
+}
+
+__device__ __forceinline__ void w512_load(double2 (&v)[8], const double2* __restrict__ buf, int t)
+{
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = buf[swz64(t + 64 * q)];
+}
+
+// One length-512 transform, layout S -> T (IN_T false) or T -> S (IN_T true),
+// X_k = sum_j x_j exp(SG 2 pi i jk/512), unscaled.  tab: the W tables
+// (twN + w512_table_offset(1024)).
+template <int SG, bool IN_T, class SY>
+__device__ __forceinline__ void dft_w512(double2 (&v)[8], double2* __restrict__ b0, double2* __restrict__ b1, int t,
+                                         const double2* __restrict__ tab, const SY& gsy, const volatile int* zero)
+{
+    const int zoff = *zero;
+    double2 ta[7], tb[8];
+    dft8<SG>(v);
+    w512_fetch_a<SG, IN_T>(ta, t, tab, zoff);
+    if constexpr (!IN_T) {
+        w512_store(v, b0, t, true);
+        gsy.sync();
+    } else {
+        __syncwarp();
+        w512_store(v, b0, t, false);
+        __syncwarp();
+    }
+    w512_load(v, b0, t);
+#pragma unroll
+    for (int q = 1; q < 8; ++q) v[q] = cmul(v[q], ta[q - 1]);
+    dft8<SG>(v);
+    w512_fetch_b<SG, IN_T>(tb, t, tab, zoff);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = cmul(v[r], tb[r]);
+    if constexpr (!IN_T) {
+        __syncwarp();
+        w512_store(v, b0, t, false);
+        __syncwarp();
+        w512_load(v, b0, t);
+    } else {
+        w512_store(v, b1, t, true);
+        gsy.sync();
+        w512_load(v, b1, t);
+    }
+    dft8<SG>(v);
+}
+
+// Two independent length-512 transforms of the same direction and layout in
+// one set of passes (v through b0/b1, u through c0/c1).
+template <int SG, bool IN_T, class SY>
+__device__ __forceinline__ void dft_w512_2(double2 (&v)[8], double2 (&u)[8], double2* __restrict__ b0,
+                                           double2* __restrict__ b1, double2* __restrict__ c0,
+                                           double2* __restrict__ c1, int t, const double2* __restrict__ tab,
+                                           const SY& gsy, const volatile int* zero)
+{
+    const int zoff = *zero;
+    double2 tw[8];
+    dft8<SG>(v);
+    dft8<SG>(u);
+    if constexpr (!IN_T) {
+        w512_store(v, b0, t, true);
+        w512_store(u, c0, t, true);
+        gsy.sync();
+    } else {
+        __syncwarp();
+        w512_store(v, b0, t, false);
+        w512_store(u, c0, t, false);
+        __syncwarp();
+    }
+    {
+        double2 ta[7];
+        w512_fetch_a<SG, IN_T>(ta, t, tab, zoff);
+        w512_load(v, b0, t);
+        w512_load(u, c0, t);
+#pragma unroll
+        for (int q = 1; q < 8; ++q) {
+            v[q] = cmul(v[q], ta[q - 1]);
+            u[q] = cmul(u[q], ta[q - 1]);
+        }
+    }
+    dft8<SG>(v);
+    dft8<SG>(u);
+    w512_fetch_b<SG, IN_T>(tw, t, tab, zoff);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        v[r] = cmul(v[r], tw[r]);
+        u[r] = cmul(u[r], tw[r]);
+    }
+    if constexpr (!IN_T) {
+        __syncwarp();
+        w512_store(v, b0, t, false);
+        w512_store(u, c0, t, false);
+        __syncwarp();
+        w512_load(v, b0, t);
+        w512_load(u, c0, t);
+    } else {
+        w512_store(v, b1, t, true);
+        w512_store(u, c1, t, true);
+        gsy.sync();
+        w512_load(v, b1, t);
+        w512_load(u, c1, t);
+    }
+    dft8<SG>(v);
+    dft8<SG>(u);
+}
+
 // --------------------------------------------------------------- slot maps
 // Slot sigma = 2*ri + parity; ri -> position q in {0, 1, 6, 7}; parity 0 odd
 // modes, 1 even modes.  Returns the state mode index (0..M-1).
@@ -404,7 +599,7 @@ __device__ __forceinline__ int slot_q(int sigma)
 // DUAL: the three pairs of independent transforms (U+iV with F, the last IA2
 // transform with dU+idV, the odd with the even forward transform) run as
 // paired transforms (dft_m2) through the second exchange pair c0/c1.
-template <int N, bool DUAL, class SY>
+template <int N, bool DUAL, bool WX, class SY>
 __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double* __restrict__ uvs, double x,
                                          double dim, double dm2c, double k0, int t, double2* __restrict__ b0,
                                          double2* __restrict__ b1, double2* __restrict__ c0,
@@ -414,6 +609,10 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
 {
     constexpr int M = N / 2, TG = M / 8;
     constexpr double invM = 1.0 / M;
+    static_assert(!WX || (M == 512 && DUAL), "warp-exchange transforms: Ntau 1024, paired");
+    // warp-exchange transforms: fixed buffer roles, the stage RHS goes to b1
+    if constexpr (WX) cur = 1;
+    const double2* __restrict__ wtab = twN + w512_table_offset(N);
     double2 v[8];
     double F[8];
     double* Us = uvs;      // [q][t], this thread's own entries only
@@ -449,7 +648,11 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
     // exchange barrier they held 32 registers through the heaviest pass
     // (1.5 % slower per C3 build, measured A/B)
     double2 pj[8];
-    if constexpr (DUAL) {
+    if constexpr (WX) {
+        even_input(u);
+        dft_w512_2<-1, false>(v, u, b0, b1, c0, c1, t, wtab, sy, zero);
+        fetch_point_twiddles_t(pj, t, twN, *zero);
+    } else if constexpr (DUAL) {
         even_input(u);
         dft_m2<M, TG, -1>(v, u, b0, b1, c0, c1, cur, t, twN, sy, active, zero);
         if (active) fetch_point_twiddles<TG>(pj, t, twN, *zero);
@@ -487,7 +690,10 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
     }
 
     // --- solveInhom (SpectralTransformer.cpp:264-292) on half-period data ----
-    dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
+    if constexpr (WX)
+        dft_w512<1, true>(v, b0, b1, t, wtab, sy, zero);
+    else
+        dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = make_double2(v[q].x * invM, v[q].y * invM);
     if (active && t == 0) *lam_slot = v[0].x;  // lambda = f_hat[0] (real: imag is exactly 0)
@@ -506,7 +712,10 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
         v[0] = make_double2(0.0, 0.0);
         v[4] = make_double2(0.0, 0.0);
     }
-    dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
+    if constexpr (WX)
+        dft_w512<-1, false>(v, b0, b1, t, wtab, sy, zero);
+    else
+        dft_m<M, TG, -1>(v, b0, b1, cur, t, twN, sy, active, zero);
     double Fr[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -524,7 +733,10 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
     // (lambda + 0i) / (lambda^2 + s^2 + 0i), s = k0 N/2 (Smith's method in
     // std::complex division), which is lambda / (lambda^2 + s^2) exactly
     const double qn = lam / (lam * lam - 0.0 * 0.0 + (k0 * N / 2.0) * (k0 * N / 2.0));
-    dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
+    if constexpr (WX)
+        dft_w512<1, true>(v, b0, b1, t, wtab, sy, zero);
+    else
+        dft_m<M, TG, 1>(v, b0, b1, cur, t, twN, sy, active, zero);
     {
         // out_k = h_k / (lambda - i s) = h_k (lambda + i s) / (lambda^2 + s^2), s = m k0,
         // with the DC and Nyquist rules of lamIntegrate for thread 0's q = 0 and
@@ -564,7 +776,15 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
         }
     };
     double IA2[8];
-    if constexpr (DUAL) {
+    if constexpr (WX) {
+        du_input(u);
+        dft_w512_2<-1, false>(v, u, b0, b1, c0, c1, t, wtab, sy, zero);
+        fetch_point_twiddles_t(pj, t, twN, *zero);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) IA2[q] = v[q].x * Fr[q];  // X e^{-F}
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = u[q];
+    } else if constexpr (DUAL) {
         du_input(u);
         dft_m2<M, TG, -1>(v, u, b0, b1, c0, c1, cur, t, twN, sy, active, zero);
         if (active) fetch_point_twiddles<TG>(pj, t, twN, *zero);
@@ -621,7 +841,15 @@ __device__ __forceinline__ void rhs_eval(const double2* __restrict__ yks, double
             fslot[7 * TG + t] = make_double2(ev[7].x * invM, ev[7].y * invM);
         }
     };
-    if constexpr (DUAL) {
+    if constexpr (WX) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) u[q] = make_double2(0.0, fx[q]);
+        dft_w512_2<1, true>(v, u, b0, b1, c0, c1, t, wtab, sy, zero);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = make_double2(v[q].x * invM, v[q].y * invM);
+        __syncwarp();  // the last exchange's reads of b1 are done before the RHS goes there
+        write_f(v, u);
+    } else if constexpr (DUAL) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) u[q] = make_double2(0.0, fx[q]);
         dft_m2<M, TG, 1>(v, u, b0, b1, c0, c1, cur, t, twN, sy, active, zero);
@@ -662,7 +890,7 @@ __device__ __forceinline__ double sweep_sum(double x, double* red, int lt, const
 
 // ------------------------------------------------------------ sweep slot
 // Shared-memory partition and thread roles of one sweep slot of a CTA.
-template <int N, int S, bool PAIR = true>
+template <int N, int S, int PAIR = 1>
 struct Slot {
     using K = MarchShape<N, S, PAIR>;
     double2* ex;    // [S][2][MP]; the stage RHS lands in one buffer of each pair
@@ -741,7 +969,7 @@ struct Slot {
 };
 
 // state -> slots: y (group 0) and every stage value (its own group)
-template <int N, int S, bool PAIR>
+template <int N, int S, int PAIR>
 __device__ __forceinline__ void load_state(const Slot<N, S, PAIR>& sl, const double* __restrict__ yin)
 {
     constexpr int TG = MarchShape<N, S, PAIR>::TG;
@@ -791,7 +1019,7 @@ struct ParamScalars {
 // The caller has loaded the state (load_state) and synchronised.  Outputs
 // are addressed through sc only where they are written, so that no output
 // pointer stays live across the march.
-template <int N, int S, bool PAIR, class SC>
+template <int N, int S, int PAIR, class SC>
 __device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S, PAIR>& sl, double k0, int side, int item,
                                            unsigned long long& n_its, unsigned long long& n_steps)
 {
@@ -882,7 +1110,7 @@ __device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S, PAIR>&
         const int max_its = sc.max_its();
         for (int its = 0; its < max_its; ++its) {
             ++its_reached;
-            rhs_eval<N, K::DUAL>(ykm, sl.uvm, xs, sc.dim(), sc.dm2c(), k0, t, sl.b0, sl.b1, sl.c0, sl.c1, cur,
+            rhs_eval<N, K::DUAL, K::WX>(ykm, sl.uvm, xs, sc.dim(), sc.dm2c(), k0, t, sl.b0, sl.b1, sl.c0, sl.c1, cur,
                                  &sl.lam[s], sc.twN(), sl.gsy, active, sl.zero);
             sl.sy.sync();  // every stage RHS is in shared memory
             double part = 0.0;
@@ -981,7 +1209,7 @@ __device__ __forceinline__ int march_item_of(int w, const MarchParams& P)
     return w < h ? 2 * w + 1 : 2 * (w - h);
 }
 
-template <int N, int S, int MINB, bool PAIR>
+template <int N, int S, int MINB, int PAIR>
 __global__ void __launch_bounds__(MarchShape<N, S, PAIR>::NT, MINB) march_kernel(MarchParams P)
 {
     using K = MarchShape<N, S, PAIR>;
@@ -1008,7 +1236,7 @@ __global__ void __launch_bounds__(MarchShape<N, S, PAIR>::NT, MINB) march_kernel
         if (P.mode == 1) {
             // single RHS evaluation of the state at x_in[item]
             int cur = 0;
-            rhs_eval<N, K::DUAL>(sl.ykm, sl.uvm, P.x_in[item], P.dim, P.dim_m2_cubed, k0, sl.t, sl.b0, sl.b1,
+            rhs_eval<N, K::DUAL, K::WX>(sl.ykm, sl.uvm, P.x_in[item], P.dim, P.dim_m2_cubed, k0, sl.t, sl.b0, sl.b1,
                                  sl.c0, sl.c1, cur, &sl.lam[sl.s], P.twN, sl.gsy, sl.active, sl.zero);
             sl.sy.sync();
             if (sl.active && sl.s == 0) {

@@ -132,6 +132,17 @@ std::vector<double2> twiddles(int n)
                 for (int k = 0; k < ns; ++k) tab[(r - 1) * ns + k] = tw[2 * (r * k * (M / (ns * R)))];
         }
     }
+    if (n == 1024 && (int)tw.size() >= w512_table_offset(n) + kW512Tables) {
+        // the warp-exchange length-512 tables (march.cuh): exp(+2 pi i e/512) = tw[2 e mod 1024]
+        double2* w = tw.data() + w512_table_offset(n);
+        for (int k = 0; k < 8; ++k)
+            for (int q = 0; q < 8; ++q) w[k * 8 + q] = tw[16 * ((q * k) % 64)];
+        for (int r = 0; r < 8; ++r)
+            for (int t = 0; t < 64; ++t) {
+                w[64 + r * 64 + t] = tw[2 * (((t & 7) * ((t >> 3) + 8 * r)) % 512)];
+                w[64 + 512 + r * 64 + t] = tw[2 * (((t >> 3) * ((t & 7) + 8 * r)) % 512)];
+            }
+    }
     return tw;
 }
 
@@ -382,7 +393,7 @@ void ensure_march_tuned(pcc_ctx* ctx, int ntau, int stages, const double2* d_tw,
             if (!std::getline(is, dev, '\t')) continue;
             if (!(is >> n >> s >> pair >> mp >> ms)) continue;
             if (dev == name && n == ntau && s == stages) {
-                march_set_tuning(ctx->device, ntau, stages, MarchTuning{pair, 0.0, 0.0});
+                march_set_tuning(ctx->device, ntau, stages, MarchTuning{pair, 0.0, 0.0, 0.0});
                 return;
             }
         }
@@ -395,7 +406,9 @@ void ensure_march_tuned(pcc_ctx* ctx, int ntau, int stages, const double2* d_tw,
     std::error_code ec;
     std::filesystem::create_directories(std::filesystem::path(path).parent_path(), ec);
     std::ofstream out(path, std::ios::app);
-    if (out) out << name << '\t' << ntau << ' ' << stages << ' ' << t.pair << ' ' << t.ms_pair << ' ' << t.ms_single << '\n';
+    if (out)
+        out << name << '\t' << ntau << ' ' << stages << ' ' << t.pair << ' ' << t.ms_pair << ' ' << t.ms_single << ' '
+            << t.ms_wx << '\n';
 }
 
 // One persistent launch over the sweeps of columns [0, ncols[i]) of every
@@ -506,7 +519,7 @@ size_t solve_footprint(const pcc_solve_desc& d, int sms)
     return ngrid * dbl + twiddle_count(n) * sizeof(double2) + 2 * nn * dbl + nn * nn * dbl + 2 * (2 * cols * n * dbl) +
            cols * nn * dbl + 2 * (2 * cols * in) + cols * in + 4 * in + 4 * sizeof(unsigned long long) +
            (size_t)2 * sms * kBoundaryArrays * n * dbl + 2 * cols * in + 4 * cols * dbl + 2 * cols * in +
-           sizeof(NewtonDev) + 3 * nn * dbl + nn * in + 2 * in + lu_mixed_work_bytes((int)nn) + in;
+           sizeof(NewtonDev) + 3 * nn * dbl + nn * in + 4 * in + lu_mixed_work_bytes((int)nn) + in;
 }
 
 pcc_status solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, cudaStream_t alloc_st, bool registered,
@@ -561,7 +574,7 @@ pcc_status solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, cudaStream_t a
     ALLOC(s->d_rhs, nn * sizeof(double));
     ALLOC(s->d_dx, nn * sizeof(double));
     ALLOC(s->d_ipiv, nn * sizeof(int));
-    ALLOC(s->d_info, 2 * sizeof(int));
+    ALLOC(s->d_info, 4 * sizeof(int));  // singular index, fell back, tensor-core wait error
     ALLOC(s->d_luw, lu_mixed_work_bytes(nn));
     ALLOC(s->d_cancel, sizeof(int));
 #undef ALLOC
@@ -1188,6 +1201,7 @@ pcc_status pcc_lu_solve(pcc_ctx* ctx, int n, const double* A, const double* rhs,
 {
     if (!ctx || n < 1 || !A || !rhs || !x) return PCC_ERR_INVALID_ARG;
     if (prec != PCC_PREC_FP64 && prec != PCC_PREC_MIXED) return PCC_ERR_INVALID_ARG;
+    if (n > lu_max_order()) return fail(ctx, PCC_ERR_INVALID_ARG, "pcc_lu_solve: n above " + std::to_string(lu_max_order()));
     PCC_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     const size_t nb = (size_t)n * n * sizeof(double);
@@ -1435,7 +1449,7 @@ pcc_status pcc_march_tuning(pcc_ctx* ctx, int ntau, int stages, int* pair, doubl
         if (e == cudaSuccess) ensure_march_tuned(ctx, ntau, stages, d_tw, ctx->stream);
         cudaFree(d_tw);
         if (e != cudaSuccess) return fail(ctx, PCC_ERR_CUDA, cudaGetErrorString(e));
-        if (!march_tuning(ctx->device, ntau, stages, &t)) t = MarchTuning{1, 0.0, 0.0};  // tuning disabled
+        if (!march_tuning(ctx->device, ntau, stages, &t)) t = MarchTuning{1, 0.0, 0.0, 0.0};  // tuning disabled
     }
     *pair = t.pair;
     if (ms_pair) *ms_pair = t.ms_pair;

@@ -46,13 +46,14 @@ bool march_supported(int ntau, int stages);
 // The autotuned transform schedule of the march for one (device, Ntau,
 // stages): paired transforms (dft_m2) or single ones, with the probe times.
 struct MarchTuning {
-    int pair;          // 1 paired, 0 single
-    double ms_pair;    // probe time of each schedule (ms), 0 when set from a cache
+    int pair;          // 0 single, 1 paired, 2 paired with the warp-exchange transforms (Ntau 1024)
+    double ms_pair;    // probe time of each schedule (ms), 0 when set from a cache or not available
     double ms_single;
+    double ms_wx;
 };
 bool march_tuning(int device, int ntau, int stages, MarchTuning* out);
 void march_set_tuning(int device, int ntau, int stages, const MarchTuning& t);
-// Times both schedules on the current device and records the faster one.
+// Times the schedules on the current device and records the choice.
 cudaError_t march_autotune(int ntau, int stages, const double2* tw, cudaStream_t st, MarchTuning* out);
 
 // Sweeps of several solves in one persistent launch (march_batch_kernel):
@@ -93,6 +94,7 @@ cudaError_t lu_solve_mixed(const double* dA, const double* db, double* dx, int n
                            int* ipiv, int* info, int max_refine, double tol, int* steps_out, double* resid_out,
                            cudaStream_t st);
 size_t lu_mixed_work_bytes(int n);
+int lu_max_order();  // largest n the LU takes (its panel lives in shared memory)
 
 cudaError_t fp64_peak_probe(double* tflops, cudaStream_t st);
 
