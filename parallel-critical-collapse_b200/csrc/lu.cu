@@ -15,7 +15,7 @@
 //                     kind::tf32 with the FP32 operands split into a TF32 high
 //                     and low part: hi*hi + hi*lo + lo*hi accumulated in FP32
 //                     in Tensor Memory, which keeps FP32 accuracy).
-// The solve with the factors (dgetrs) is one CTA: row swaps, then unit-lower
+// The solve with the factors (dgetrs) is one CTA: the row permutation, then unit-lower
 // forward and upper backward substitution in blocks of 32 (one warp solves a
 // diagonal block with shuffles, the CTA updates the other rows).
 //
@@ -51,22 +51,35 @@ int panel_nb(int n, size_t es)
     return nb;
 }
 
-template <typename T>
+// nb <= NB: the panel's width (NB, or less for the last panel of a matrix
+// whose order is not a multiple of NB).
+template <typename T, int NB>
 __global__ void __launch_bounds__(kPanelThreads) panel_kernel(T* A, int n, int k0, int nb, int* ipiv, int* info)
 {
     extern __shared__ __align__(16) unsigned char panel_smem[];
-    T* P = reinterpret_cast<T*>(panel_smem);  // [m][nb + 1]
-    constexpr int NW = kPanelThreads / 32;
+    T* P = reinterpret_cast<T*>(panel_smem);  // [m][NB + 1]
+    constexpr int NW = kPanelThreads / 32, ld = NB + 1;
+    static_assert(NW <= 32, "one warp reduces the warps' candidates");
     __shared__ T s_val[NW];
     __shared__ int s_idx[NW];
-    const int m = n - k0, ld = nb + 1, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int m = n - k0, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int e = tid; e < m * nb; e += kPanelThreads) {
         const int r = e / nb, c = e - r * nb;
         P[r * ld + c] = A[(size_t)(k0 + r) * n + k0 + c];
     }
     __syncthreads();
+    auto argmax = [](T& best, int& bi, int width) {
+        for (int o = width / 2; o > 0; o >>= 1) {
+            const T ov = __shfl_down_sync(0xffffffffu, best, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
+            }
+        }
+    };
     for (int j = 0; j < nb && j < m; ++j) {
-        // pivot: the first row of maximal |P[r][j]|, r >= j
+        // pivot: the first row of maximal |P[r][j]|, r >= j (ties: the smaller row, as idamax)
         T best = T(-1);
         int bi = j;
         for (int r = j + tid; r < m; r += kPanelThreads) {
@@ -76,29 +89,17 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(T* A, int n, int k
                 bi = r;
             }
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            const T ov = __shfl_down_sync(0xffffffffu, best, o);
-            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-            if (ov > best || (ov == best && oi < bi)) {
-                best = ov;
-                bi = oi;
-            }
-        }
+        argmax(best, bi, 32);
         if (lane == 0) {
             s_val[warp] = best;
             s_idx[warp] = bi;
         }
         __syncthreads();
-        T pb = s_val[0];
-        int p = s_idx[0];
-        for (int w = 1; w < NW; ++w) {
-            const T v = s_val[w];
-            const int i = s_idx[w];
-            if (v > pb || (v == pb && i < p)) {
-                pb = v;
-                p = i;
-            }
-        }
+        T pb = lane < NW ? s_val[lane] : T(-1);
+        int p = lane < NW ? s_idx[lane] : 0x7fffffff;
+        argmax(pb, p, 32);
+        pb = __shfl_sync(0xffffffffu, pb, 0);
+        p = __shfl_sync(0xffffffffu, p, 0);
         if (p != j && tid < nb) {
             const T t = P[j * ld + tid];
             P[j * ld + tid] = P[p * ld + tid];
@@ -112,10 +113,15 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(T* A, int n, int k
         const T piv = P[j * ld + j];
         if (piv != T(0)) {
             const T rcp = T(1) / piv;
+            T prow[NB];
+#pragma unroll
+            for (int c = 0; c < NB; ++c) prow[c] = P[j * ld + c];
             for (int r = j + 1 + tid; r < m; r += kPanelThreads) {
                 const T l = P[r * ld + j] * rcp;
                 P[r * ld + j] = l;
-                for (int c = j + 1; c < nb; ++c) P[r * ld + c] -= l * P[j * ld + c];
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+                    if (c > j && c < nb) P[r * ld + c] -= l * prow[c];
             }
         }
         __syncthreads();
@@ -124,6 +130,30 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(T* A, int n, int k
         const int r = e / nb, c = e - r * nb;
         A[(size_t)(k0 + r) * n + k0 + c] = P[r * ld + c];
     }
+}
+
+// The row interchanges of the whole factorisation as one permutation: the
+// LAPACK pivot sequence (row i swapped with ipiv[i], i = 0..n-1) applied to
+// the identity, so that (P b)[i] = b[perm[i]].  One warp; written over ipiv.
+__global__ void perm_kernel(int* ipiv, int n)
+{
+    extern __shared__ int perm_smem[];
+    int* piv = perm_smem;
+    int* idx = perm_smem + n;
+    for (int i = threadIdx.x; i < n; i += 32) {
+        piv[i] = ipiv[i];
+        idx[i] = i;
+    }
+    __syncwarp();
+    if (threadIdx.x == 0)
+        for (int i = 0; i < n; ++i) {
+            const int p = piv[i];
+            const int t = idx[i];
+            idx[i] = idx[p];
+            idx[p] = t;
+        }
+    __syncwarp();
+    for (int i = threadIdx.x; i < n; i += 32) ipiv[i] = idx[i];
 }
 
 // The panel's interchanges on every column outside it (dlaswp, in pivot
@@ -224,8 +254,8 @@ __global__ void __launch_bounds__(256) update_kernel(T* A, int n, int k0, int nb
 // accumulator in Tensor Memory receives hi*hi + hi*lo + lo*hi, which keeps the
 // product to about FP32 accuracy (the lo*lo term is below it).  One thread
 // issues the MMAs and commits them to an mbarrier; after a bounded wait every
-// warp reads its 32 lanes of the 128 x 128 FP32 accumulator (tcgen05.ld) and
-// subtracts them from A22.
+// warp reads its 32 lanes of the 128 x 128 FP32 accumulator (tcgen05.ld) into
+// shared memory, and the CTA subtracts the tile from A22 row by row.
 constexpr int kTcM = 128, kTcN = 128;
 constexpr uint32_t kTcCols = 128;            // TMEM columns allocated (N FP32 accumulators)
 constexpr long long kTcWaitLimit = 1 << 24;  // mbarrier polls before giving up
@@ -355,11 +385,15 @@ __global__ void __launch_bounds__(128) tc_update_kernel(float* A, int n, int k0,
         done = ok != 0;
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!done) {
+    // every thread saw the MMAs complete (else none reads the accumulator)
+    const bool all_done = __syncthreads_and(done) != 0;
+    float* stage = reinterpret_cast<float*>(tc_smem);  // [128][129]: the operands are no longer read
+    if (!all_done) {
         if (tid == 0) atomicExch(err, 1);
     } else {
-        // this warp's 32 lanes = rows 32 warp + lane of the tile
-        const int row = r0 + 32 * warp + lane;
+        // this warp's 32 lanes = rows 32 warp + lane of the tile, through
+        // shared memory so that the update of A22 below is row-coalesced
+        const int lrow = 32 * warp + lane;
 #pragma unroll 1
         for (int cb = 0; cb < kTcN; cb += 32) {
             uint32_t v[32];
@@ -375,12 +409,16 @@ __global__ void __launch_bounds__(128) tc_update_kernel(float* A, int n, int k0,
                   "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < n) {
-                float* crow = A + (size_t)row * n + c0 + cb;
 #pragma unroll
-                for (int j = 0; j < 32; ++j)
-                    if (c0 + cb + j < n) crow[j] -= __uint_as_float(v[j]);
-            }
+            for (int j = 0; j < 32; ++j) stage[lrow * (kTcN + 1) + cb + j] = __uint_as_float(v[j]);
+        }
+    }
+    __syncthreads();
+    if (all_done) {
+        const int col = c0 + tid;
+        for (int rr = 0; rr < kTcM; ++rr) {
+            const int row = r0 + rr;
+            if (row < n && col < n) A[(size_t)row * n + col] -= stage[rr * (kTcN + 1) + tid];
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -418,7 +456,8 @@ cudaError_t launch_tc_update(float* A, int n, int k0, int nb, int* err, cudaStre
 {
     const int rest = n - k0 - nb;
     dim3 g((rest + kTcN - 1) / kTcN, (rest + kTcM - 1) / kTcM);
-    const size_t smem = 4 * (size_t)kTcM * nb * sizeof(float);
+    const size_t ops = 4 * (size_t)kTcM * nb * sizeof(float), stage = (size_t)kTcM * (kTcN + 1) * sizeof(float);
+    const size_t smem = ops > stage ? ops : stage;
     cudaError_t e = cudaSuccess;
     switch (nb) {
         case 32:
@@ -439,7 +478,8 @@ cudaError_t launch_tc_update(float* A, int n, int k0, int nb, int* err, cudaStre
 }
 
 // info[0]: 1-based index of the first zero pivot (0: none); info[2]: the
-// tensor-core update gave up waiting (then the factors are not used).
+// tensor-core update gave up waiting (then the factors are not used).  On
+// return ipiv holds the row permutation (perm_kernel), not LAPACK's pivots.
 template <typename T>
 cudaError_t lu_factor(T* A, int n, int* ipiv, int* info, bool tc, cudaStream_t st)
 {
@@ -448,12 +488,13 @@ cudaError_t lu_factor(T* A, int n, int* ipiv, int* info, bool tc, cudaStream_t s
     const int nb_max = panel_nb(n, sizeof(T));
     const size_t psmem_max = (size_t)n * (nb_max + 1) * sizeof(T);
     if (psmem_max > kPanelSmemCap) return cudaErrorInvalidValue;  // n above lu_max_order()
-    e = cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem_max);
+    auto panel = nb_max == 32 ? panel_kernel<T, 32> : nb_max == 16 ? panel_kernel<T, 16> : panel_kernel<T, 8>;
+    e = cudaFuncSetAttribute(panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem_max);
     if (e != cudaSuccess) return e;
     for (int k0 = 0; k0 < n; k0 += nb_max) {
         const int nb = n - k0 < nb_max ? n - k0 : nb_max;
-        const size_t psmem = (size_t)(n - k0) * (nb + 1) * sizeof(T);
-        panel_kernel<T><<<1, kPanelThreads, psmem, st>>>(A, n, k0, nb, ipiv, info);
+        const size_t psmem = (size_t)(n - k0) * (nb_max + 1) * sizeof(T);
+        panel<<<1, kPanelThreads, psmem, st>>>(A, n, k0, nb, ipiv, info);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         if ((e = launch_swap_trsm<T>(A, n, k0, nb, nb_max, ipiv, st)) != cudaSuccess) return e;
         const int rest = n - k0 - nb;
@@ -470,17 +511,18 @@ cudaError_t lu_factor(T* A, int n, int* ipiv, int* info, bool tc, cudaStream_t s
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
     }
-    return cudaSuccess;
+    perm_kernel<<<1, 32, 2 * (size_t)n * sizeof(int), st>>>(ipiv, n);
+    return cudaGetLastError();
 }
 
-// x = A^{-1} b from the factors (dgetrs): row swaps, unit-lower forward and
-// upper backward substitution in blocks of 32.  One CTA of 512 threads; x
+// x = A^{-1} b from the factors (dgetrs): the row permutation (a gather),
+// unit-lower forward and upper backward substitution in blocks of 32.  One CTA of 512 threads; x
 // lives in shared memory (n TB values).  skip: optional device flag; a
 // nonzero value makes the call return at once (the refinement loop's "done").
 constexpr int kGetrsThreads = 512;
 
 template <typename T, typename TB>
-__global__ void __launch_bounds__(kGetrsThreads) getrs_kernel(const T* A, int n, const int* ipiv, const TB* b, TB* x,
+__global__ void __launch_bounds__(kGetrsThreads) getrs_kernel(const T* A, int n, const int* perm, const TB* b, TB* x,
                                                               const int* skip)
 {
     if (skip && *(const volatile int*)skip) return;
@@ -488,17 +530,7 @@ __global__ void __launch_bounds__(kGetrsThreads) getrs_kernel(const T* A, int n,
     TB* xs = reinterpret_cast<TB*>(getrs_smem);
     constexpr int NT = kGetrsThreads, NWS = NT / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < n; i += NT) xs[i] = b[i];
-    __syncthreads();
-    if (tid == 0)
-        for (int i = 0; i < n; ++i) {
-            const int p = ipiv[i];
-            if (p != i) {
-                const TB t = xs[i];
-                xs[i] = xs[p];
-                xs[p] = t;
-            }
-        }
+    for (int i = tid; i < n; i += NT) xs[i] = b[perm[i]];  // P b
     __syncthreads();
     // forward: L y = P b, L unit lower
     for (int jb = 0; jb < n; jb += 32) {
