@@ -78,7 +78,9 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(T* A, int n, int k
             }
         }
     };
-    for (int j = 0; j < nb && j < m; ++j) {
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        if (j >= nb || j >= m) break;
         // pivot: the first row of maximal |P[r][j]|, r >= j (ties: the smaller row, as idamax)
         T best = T(-1);
         int bi = j;
@@ -115,13 +117,12 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(T* A, int n, int k
             const T rcp = T(1) / piv;
             T prow[NB];
 #pragma unroll
-            for (int c = 0; c < NB; ++c) prow[c] = P[j * ld + c];
+            for (int c = j + 1; c < NB; ++c) prow[c] = c < nb ? P[j * ld + c] : T(0);
             for (int r = j + 1 + tid; r < m; r += kPanelThreads) {
                 const T l = P[r * ld + j] * rcp;
                 P[r * ld + j] = l;
 #pragma unroll
-                for (int c = 0; c < NB; ++c)
-                    if (c > j && c < nb) P[r * ld + c] -= l * prow[c];
+                for (int c = j + 1; c < NB; ++c) P[r * ld + c] -= l * prow[c];
             }
         }
         __syncthreads();
@@ -230,16 +231,21 @@ __global__ void __launch_bounds__(256) update_kernel(T* A, int n, int k0, int nb
 #pragma unroll
             for (int v = 0; v < 4; ++v) acc[u][v] += a[u] * b[v];
     }
+    T old[4][4];  // all sixteen loads in flight before the stores
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int r = r0 + ty + 16 * u;
-        if (r >= n) continue;
+    for (int u = 0; u < 4; ++u)
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            const int c = c0 + tx + 16 * v;
-            if (c < n) A[(size_t)r * n + c] -= acc[u][v];
+            const int r = r0 + ty + 16 * u, c = c0 + tx + 16 * v;
+            old[u][v] = (r < n && c < n) ? A[(size_t)r * n + c] : T(0);
         }
-    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int r = r0 + ty + 16 * u, c = c0 + tx + 16 * v;
+            if (r < n && c < n) A[(size_t)r * n + c] = old[u][v] - acc[u][v];
+        }
 }
 
 // ------------------------------------------------------------------------
@@ -414,11 +420,15 @@ __global__ void __launch_bounds__(128) tc_update_kernel(float* A, int n, int k0,
         }
     }
     __syncthreads();
-    if (all_done) {
+    if (all_done && c0 + tid < n) {
         const int col = c0 + tid;
-        for (int rr = 0; rr < kTcM; ++rr) {
-            const int row = r0 + rr;
-            if (row < n && col < n) A[(size_t)row * n + col] -= stage[rr * (kTcN + 1) + tid];
+        for (int rr0 = 0; rr0 < kTcM; rr0 += 8) {
+            float a[8];  // eight rows' loads in flight together
+#pragma unroll
+            for (int u = 0; u < 8; ++u) a[u] = r0 + rr0 + u < n ? A[(size_t)(r0 + rr0 + u) * n + col] : 0.0f;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (r0 + rr0 + u < n) A[(size_t)(r0 + rr0 + u) * n + col] = a[u] - stage[(rr0 + u) * (kTcN + 1) + tid];
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -521,6 +531,29 @@ cudaError_t lu_factor(T* A, int n, int* ipiv, int* info, bool tc, cudaStream_t s
 // nonzero value makes the call return at once (the refinement loop's "done").
 constexpr int kGetrsThreads = 512;
 
+// xs[i] -= sum_l A[i][jb + l] xs[jb + l], l < bw, for rows i in [i_lo, i_hi):
+// one warp per group of 8 rows, lanes across the block's columns, the 8 rows'
+// loads issued together so that their latencies overlap.
+template <typename T, typename TB>
+__device__ __forceinline__ void block_gemv(const T* __restrict__ A, int n, TB* xs, int jb, int bw, int i_lo,
+                                           int i_hi, int lane, int warp, int nwarps)
+{
+    const TB xj = lane < bw ? xs[jb + lane] : TB(0);
+    for (int i0 = i_lo + 8 * warp; i0 < i_hi; i0 += 8 * nwarps) {
+        TB s[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            s[u] = (i0 + u < i_hi && lane < bw) ? (TB)A[(size_t)(i0 + u) * n + jb + lane] * xj : TB(0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int u = 0; u < 8; ++u) s[u] += __shfl_xor_sync(0xffffffffu, s[u], o);
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (lane == u && i0 + u < i_hi) xs[i0 + u] -= s[u];
+    }
+}
+
 template <typename T, typename TB>
 __global__ void __launch_bounds__(kGetrsThreads) getrs_kernel(const T* A, int n, const int* perm, const TB* b, TB* x,
                                                               const int* skip)
@@ -549,12 +582,7 @@ __global__ void __launch_bounds__(kGetrsThreads) getrs_kernel(const T* A, int n,
             if (lane < bw) xs[jb + lane] = xv;
         }
         __syncthreads();
-        for (int i = jb + bw + warp; i < n; i += NWS) {
-            TB s = lane < bw ? (TB)A[(size_t)i * n + jb + lane] * xs[jb + lane] : TB(0);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) xs[i] -= s;
-        }
+        block_gemv<T, TB>(A, n, xs, jb, bw, jb + bw, n, lane, warp, NWS);
         __syncthreads();
     }
     // backward: U x = y
@@ -575,12 +603,7 @@ __global__ void __launch_bounds__(kGetrsThreads) getrs_kernel(const T* A, int n,
             if (lane < bw) xs[jb + lane] = xv;
         }
         __syncthreads();
-        for (int i = warp; i < jb; i += NWS) {
-            TB s = lane < bw ? (TB)A[(size_t)i * n + jb + lane] * xs[jb + lane] : TB(0);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) xs[i] -= s;
-        }
+        block_gemv<T, TB>(A, n, xs, jb, bw, 0, jb, lane, warp, NWS);
         __syncthreads();
     }
     for (int i = tid; i < n; i += NT) x[i] = xs[i];
