@@ -610,6 +610,22 @@ def run_serving(eng, args, rate, n_req, precision="fp64"):
             "note": "percentiles over `requests` draws (with 16 the p99 is the maximum)"}
 
 
+def run_serving_only(args, local):
+    """C5 alone, for a longer measurement than the bench line carries: one
+    JSON line per (rate, precision)."""
+    import torch
+
+    import pcc
+
+    torch.cuda.set_device(local)
+    eng = pcc.Engine(local)
+    for prec, rates in (("fp64", args.rates), ("mixed", args.mixed_rates)):
+        for r in rates.split(","):
+            if r:
+                print(json.dumps({"serving": run_serving(eng, args, float(r), args.requests, prec)}), flush=True)
+    eng.close()
+
+
 def run_engine(args, world, rank, local):
     import torch
 
@@ -762,6 +778,8 @@ def main():
                          "the Jacobian's column count times a full build)")
     ap.add_argument("--columns", type=int, default=0,
                     help="profiling aid: build only the first C columns (not a benchmark line)")
+    ap.add_argument("--serving-only", action="store_true",
+                    help="only C5: one JSON line per rate (--rates FP64, --mixed-rates mixed), no bench line")
     ap.add_argument("--dry-run", action="store_true",
                     help="no GPU: the rank launch and multi-rank host logic on gloo (a test of the launcher)")
     args = ap.parse_args()
@@ -774,6 +792,8 @@ def main():
     try:
         if args.dry_run:
             run_dry(args, world, rank)
+        elif args.serving_only:
+            run_serving_only(args, local)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         elif args.shard == "columns":
