@@ -610,6 +610,31 @@ def run_serving(eng, args, rate, n_req, precision="fp64"):
             "note": "percentiles over `requests` draws (with 16 the p99 is the maximum)"}
 
 
+def run_lu_case(args, local):
+    """A profiling case for the dense solve: a seeded n x n system with
+    singular values graded from 1 to 1e-6, solved in FP64 and in mixed
+    precision; prints the refine reports and the errors against numpy's
+    LAPACK dgesv."""
+    import torch
+
+    import pcc
+
+    torch.cuda.set_device(local)
+    eng = pcc.Engine(local)
+    n = args.lu
+    rng = np.random.default_rng(768)
+    u, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    v, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    A = (u * np.logspace(0, -6, n)) @ v.T
+    b = rng.standard_normal(n)
+    xn = np.linalg.solve(A, b)
+    for prec in (pcc.PREC_FP64, pcc.PREC_MIXED):
+        x, rep = eng.lu_solve(A, b, precision=prec)
+        print(json.dumps({"lu_case": n, "precision": prec, **rep,
+                          "rel_err_vs_dgesv": float(np.linalg.norm(x - xn) / np.linalg.norm(xn))}))
+    eng.close()
+
+
 def run_serving_only(args, local):
     """C5 alone, for a longer measurement than the bench line carries: one
     JSON line per (rate, precision)."""
@@ -778,6 +803,9 @@ def main():
                          "the Jacobian's column count times a full build)")
     ap.add_argument("--columns", type=int, default=0,
                     help="profiling aid: build only the first C columns (not a benchmark line)")
+    ap.add_argument("--lu", type=int, default=0,
+                    help="profiling aid: pcc_lu_solve, FP64 then mixed, on a seeded n x n system of condition "
+                         "number 1e6 (prints the refine reports, not a benchmark line)")
     ap.add_argument("--serving-only", action="store_true",
                     help="only C5: one JSON line per rate (--rates FP64, --mixed-rates mixed), no bench line")
     ap.add_argument("--dry-run", action="store_true",
@@ -794,6 +822,8 @@ def main():
             run_dry(args, world, rank)
         elif args.serving_only:
             run_serving_only(args, local)
+        elif args.lu:
+            run_lu_case(args, local)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         elif args.shard == "columns":
