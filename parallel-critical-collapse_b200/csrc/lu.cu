@@ -53,23 +53,23 @@ int panel_nb(int n, size_t es)
 
 // nb <= NB: the panel's width (NB, or less for the last panel of a matrix
 // whose order is not a multiple of NB).
-template <typename T, int NB>
-__global__ void __launch_bounds__(kPanelThreads) panel_kernel(T* A, int n, int k0, int nb, int* ipiv, int* info)
+template <typename T, int NB, int NT>
+__global__ void __launch_bounds__(NT) panel_kernel(T* A, int n, int k0, int nb, int* ipiv, int* info)
 {
     extern __shared__ __align__(16) unsigned char panel_smem[];
     T* P = reinterpret_cast<T*>(panel_smem);  // [m][NB + 1]
-    constexpr int NW = kPanelThreads / 32, ld = NB + 1;
+    constexpr int NW = NT / 32, ld = NB + 1;
     static_assert(NW <= 32, "one warp reduces the warps' candidates");
     __shared__ T s_val[NW];
     __shared__ int s_idx[NW];
     const int m = n - k0, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int e = tid; e < m * nb; e += kPanelThreads) {
+    for (int e = tid; e < m * nb; e += NT) {
         const int r = e / nb, c = e - r * nb;
         P[r * ld + c] = A[(size_t)(k0 + r) * n + k0 + c];
     }
     __syncthreads();
-    auto argmax = [](T& best, int& bi, int width) {
-        for (int o = width / 2; o > 0; o >>= 1) {
+    auto argmax = [](T& best, int& bi) {
+        for (int o = 16; o > 0; o >>= 1) {
             const T ov = __shfl_down_sync(0xffffffffu, best, o);
             const int oi = __shfl_down_sync(0xffffffffu, bi, o);
             if (ov > best || (ov == best && oi < bi)) {
@@ -78,28 +78,32 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(T* A, int n, int k
             }
         }
     };
-#pragma unroll
-    for (int j = 0; j < NB; ++j) {
-        if (j >= nb || j >= m) break;
-        // pivot: the first row of maximal |P[r][j]|, r >= j (ties: the smaller row, as idamax)
+    // the pivot candidates of column 0; later columns' candidates are found
+    // while the previous column's update writes them (two barriers a column)
+    {
         T best = T(-1);
-        int bi = j;
-        for (int r = j + tid; r < m; r += kPanelThreads) {
-            const T v = fabs(P[r * ld + j]);
+        int bi = 0;
+        for (int r = tid; r < m; r += NT) {
+            const T v = fabs(P[r * ld]);
             if (v > best) {
                 best = v;
                 bi = r;
             }
         }
-        argmax(best, bi, 32);
+        argmax(best, bi);
         if (lane == 0) {
             s_val[warp] = best;
             s_idx[warp] = bi;
         }
         __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        if (j < nb && j < m) {  // uniform over the CTA
+        // pivot: the first row of maximal |P[r][j]|, r >= j (ties: the smaller row, as idamax)
         T pb = lane < NW ? s_val[lane] : T(-1);
         int p = lane < NW ? s_idx[lane] : 0x7fffffff;
-        argmax(pb, p, 32);
+        argmax(pb, p);
         pb = __shfl_sync(0xffffffffu, pb, 0);
         p = __shfl_sync(0xffffffffu, p, 0);
         if (p != j && tid < nb) {
@@ -113,21 +117,44 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(T* A, int n, int k
         }
         __syncthreads();
         const T piv = P[j * ld + j];
+        T best = T(-1);
+        int bi = j + 1;
         if (piv != T(0)) {
             const T rcp = T(1) / piv;
             T prow[NB];
 #pragma unroll
             for (int c = j + 1; c < NB; ++c) prow[c] = c < nb ? P[j * ld + c] : T(0);
-            for (int r = j + 1 + tid; r < m; r += kPanelThreads) {
+            for (int r = j + 1 + tid; r < m; r += NT) {
                 const T l = P[r * ld + j] * rcp;
                 P[r * ld + j] = l;
 #pragma unroll
                 for (int c = j + 1; c < NB; ++c) P[r * ld + c] -= l * prow[c];
+                if (j + 1 < NB) {
+                    const T v = fabs(P[r * ld + j + 1]);
+                    if (v > best) {
+                        best = v;
+                        bi = r;
+                    }
+                }
+            }
+        } else if (j + 1 < NB) {
+            for (int r = j + 1 + tid; r < m; r += NT) {
+                const T v = fabs(P[r * ld + j + 1]);
+                if (v > best) {
+                    best = v;
+                    bi = r;
+                }
             }
         }
+        argmax(best, bi);
+        if (lane == 0) {
+            s_val[warp] = best;
+            s_idx[warp] = bi;
+        }
         __syncthreads();
+        }
     }
-    for (int e = tid; e < m * nb; e += kPanelThreads) {
+    for (int e = tid; e < m * nb; e += NT) {
         const int r = e / nb, c = e - r * nb;
         A[(size_t)(k0 + r) * n + k0 + c] = P[r * ld + c];
     }
@@ -439,6 +466,15 @@ __global__ void __launch_bounds__(128) tc_update_kernel(float* A, int n, int k0,
     }
 }
 
+// Threads of the panel factorisation CTA ($PCC_LU_PANEL_THREADS = 128, 256
+// or 512; default 512).
+int panel_threads()
+{
+    const char* v = std::getenv("PCC_LU_PANEL_THREADS");
+    const int t = v ? std::atoi(v) : kPanelThreads;
+    return t == 128 || t == 256 ? t : kPanelThreads;
+}
+
 // 1 (default): the FP32 trailing updates run on the tensor cores; 0
 // ($PCC_LU_TC=0): on the CUDA cores (the same kernel as FP64), for comparison.
 bool lu_tensor_cores()
@@ -498,13 +534,21 @@ cudaError_t lu_factor(T* A, int n, int* ipiv, int* info, bool tc, cudaStream_t s
     const int nb_max = panel_nb(n, sizeof(T));
     const size_t psmem_max = (size_t)n * (nb_max + 1) * sizeof(T);
     if (psmem_max > kPanelSmemCap) return cudaErrorInvalidValue;  // n above lu_max_order()
-    auto panel = nb_max == 32 ? panel_kernel<T, 32> : nb_max == 16 ? panel_kernel<T, 16> : panel_kernel<T, 8>;
+    const int nt = panel_threads();
+    using PanelFn = void (*)(T*, int, int, int, int*, int*);
+    PanelFn panel;
+    if (nt == 128)
+        panel = nb_max == 32 ? panel_kernel<T, 32, 128> : nb_max == 16 ? panel_kernel<T, 16, 128> : panel_kernel<T, 8, 128>;
+    else if (nt == 256)
+        panel = nb_max == 32 ? panel_kernel<T, 32, 256> : nb_max == 16 ? panel_kernel<T, 16, 256> : panel_kernel<T, 8, 256>;
+    else
+        panel = nb_max == 32 ? panel_kernel<T, 32, 512> : nb_max == 16 ? panel_kernel<T, 16, 512> : panel_kernel<T, 8, 512>;
     e = cudaFuncSetAttribute(panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem_max);
     if (e != cudaSuccess) return e;
     for (int k0 = 0; k0 < n; k0 += nb_max) {
         const int nb = n - k0 < nb_max ? n - k0 : nb_max;
         const size_t psmem = (size_t)(n - k0) * (nb_max + 1) * sizeof(T);
-        panel<<<1, kPanelThreads, psmem, st>>>(A, n, k0, nb, ipiv, info);
+        panel<<<1, nt, psmem, st>>>(A, n, k0, nb, ipiv, info);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         if ((e = launch_swap_trsm<T>(A, n, k0, nb, nb_max, ipiv, st)) != cudaSuccess) return e;
         const int rest = n - k0 - nb;
@@ -532,24 +576,25 @@ cudaError_t lu_factor(T* A, int n, int* ipiv, int* info, bool tc, cudaStream_t s
 constexpr int kGetrsThreads = 512;
 
 // xs[i] -= sum_l A[i][jb + l] xs[jb + l], l < bw, for rows i in [i_lo, i_hi):
-// one warp per group of 8 rows, lanes across the block's columns, the 8 rows'
-// loads issued together so that their latencies overlap.
+// one warp per group of 16 rows, lanes across the block's columns, the 16
+// rows' loads issued together so that their latencies overlap.
 template <typename T, typename TB>
 __device__ __forceinline__ void block_gemv(const T* __restrict__ A, int n, TB* xs, int jb, int bw, int i_lo,
                                            int i_hi, int lane, int warp, int nwarps)
 {
+    constexpr int R = 16;
     const TB xj = lane < bw ? xs[jb + lane] : TB(0);
-    for (int i0 = i_lo + 8 * warp; i0 < i_hi; i0 += 8 * nwarps) {
-        TB s[8];
+    for (int i0 = i_lo + R * warp; i0 < i_hi; i0 += R * nwarps) {
+        TB s[R];
 #pragma unroll
-        for (int u = 0; u < 8; ++u)
+        for (int u = 0; u < R; ++u)
             s[u] = (i0 + u < i_hi && lane < bw) ? (TB)A[(size_t)(i0 + u) * n + jb + lane] * xj : TB(0);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
-            for (int u = 0; u < 8; ++u) s[u] += __shfl_xor_sync(0xffffffffu, s[u], o);
+            for (int u = 0; u < R; ++u) s[u] += __shfl_xor_sync(0xffffffffu, s[u], o);
 #pragma unroll
-        for (int u = 0; u < 8; ++u)
+        for (int u = 0; u < R; ++u)
             if (lane == u && i0 + u < i_hi) xs[i0 + u] -= s[u];
     }
 }
