@@ -71,3 +71,14 @@ def test_lu_singular_is_reported(engine):
         with pytest.raises(pcc.PccError) as e:
             engine.lu_solve(A, np.ones(96), precision=prec)
         assert e.value.status == 7
+
+
+def test_lu_order_above_limit_is_refused(engine):
+    """The factorisation panel lives in shared memory, which bounds the order
+    (3128); a larger system is refused before anything is allocated."""
+    import pcc
+
+    n = 3200
+    with pytest.raises(pcc.PccError) as e:
+        engine.lu_solve(np.eye(n), np.ones(n), precision=0)
+    assert e.value.status == pcc.PCC_ERR_INVALID_ARG

@@ -185,3 +185,42 @@ def test_serve_stop_while_waiting_and_results_delivered_once(engine):
     assert not th_w.is_alive() and not th_p.is_alive()
     assert got["r"]["done"] == 1 and got["r"]["status"] == 0 and got["x"] is not None
     assert polled["codes"] <= {pcc.PCC_ERR_INVALID_ARG}  # unknown ticket before and after the stop
+
+
+def test_first_submits_from_two_threads_start_one_loop():
+    """Serving starts lazily inside the first pcc_submit; two threads that
+    submit at the same moment on a fresh context both get their requests
+    queued (no PCC_ERR_BUSY from a second start) and both results arrive."""
+    import threading
+
+    import pcc
+
+    c1 = load_case("c1_newton")
+    cfg = _cfg(c1, PrecisionNewton=1e-12, MaxIterNewton=12)
+    eng = pcc.Engine(0)
+    try:
+        go = threading.Barrier(2)
+        tickets, errors = [], []
+
+        def submit():
+            go.wait()
+            try:
+                tickets.append(eng.submit(cfg, c1["in0"]))
+            except pcc.PccError as e:
+                errors.append(e)
+
+        ths = [threading.Thread(target=submit) for _ in range(2)]
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join(60)
+        assert not errors and len(tickets) == 2 and tickets[0] != tickets[1]
+        xs = []
+        for t in tickets:
+            r, x = eng.wait(t, 600.0)
+            assert r["done"] == 1 and r["status"] == 0
+            xs.append(x)
+        assert np.array_equal(xs[0], xs[1])
+        eng.serve_stop()
+    finally:
+        eng.close()
