@@ -172,6 +172,8 @@ def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "reference":
+        return world, rank, local  # the CPU arm: rank 0 alone works, no collective is taken
     if world > 1:
         import datetime
 
@@ -831,7 +833,7 @@ def main():
         else:
             run_engine(args, world, rank, local)
     finally:
-        if world > 1:
+        if world > 1 and args.impl != "reference":
             import torch.distributed as dist
 
             dist.destroy_process_group()
