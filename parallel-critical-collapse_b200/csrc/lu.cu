@@ -576,8 +576,9 @@ cudaError_t lu_factor(T* A, int n, int* ipiv, int* info, bool tc, cudaStream_t s
 constexpr int kGetrsThreads = 512;
 
 // xs[i] -= sum_l A[i][jb + l] xs[jb + l], l < bw, for rows i in [i_lo, i_hi):
-// one warp per group of 16 rows, lanes across the block's columns, the 16
-// rows' loads issued together so that their latencies overlap.
+// one warp per group of 16 rows (warps numbered 0..nwarps-1 among those
+// taking part), lanes across the block's columns, the 16 rows' loads issued
+// together so that their latencies overlap.
 template <typename T, typename TB>
 __device__ __forceinline__ void block_gemv(const T* __restrict__ A, int n, TB* xs, int jb, int bw, int i_lo,
                                            int i_hi, int lane, int warp, int nwarps)
@@ -609,16 +610,28 @@ __global__ void __launch_bounds__(kGetrsThreads) getrs_kernel(const T* A, int n,
     constexpr int NT = kGetrsThreads, NWS = NT / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < n; i += NT) xs[i] = b[perm[i]];  // P b
+    // Warp 0 solves the diagonal blocks; it holds the current block's row
+    // (this lane's) in registers and loads the next block's while warps
+    // 1.. update the other rows, so no load sits on the block-to-block chain.
+    T row[32];
+    auto load_lower = [&](int jb) {
+        const int bw = n - jb < 32 ? n - jb : 32;
+#pragma unroll
+        for (int l = 0; l < 32; ++l)
+            row[l] = (lane < bw && l < lane) ? A[(size_t)(jb + lane) * n + jb + l] : T(0);
+    };
+    auto load_upper = [&](int jb, int bw) {
+#pragma unroll
+        for (int l = 0; l < 32; ++l)
+            row[l] = (lane < bw && l >= lane && l < bw) ? A[(size_t)(jb + lane) * n + jb + l] : T(1);
+    };
+    if (warp == 0) load_lower(0);
     __syncthreads();
     // forward: L y = P b, L unit lower
     for (int jb = 0; jb < n; jb += 32) {
         const int bw = n - jb < 32 ? n - jb : 32;
         if (warp == 0) {
             TB xv = lane < bw ? xs[jb + lane] : TB(0);
-            T row[32];
-#pragma unroll
-            for (int l = 0; l < 32; ++l)
-                row[l] = (lane < bw && l < lane) ? A[(size_t)(jb + lane) * n + jb + l] : T(0);
 #pragma unroll
             for (int l = 0; l < 32; ++l) {
                 const TB xl = __shfl_sync(0xffffffffu, xv, l);
@@ -627,7 +640,14 @@ __global__ void __launch_bounds__(kGetrsThreads) getrs_kernel(const T* A, int n,
             if (lane < bw) xs[jb + lane] = xv;
         }
         __syncthreads();
-        block_gemv<T, TB>(A, n, xs, jb, bw, jb + bw, n, lane, warp, NWS);
+        if (warp == 0) {
+            if (jb + 32 < n)
+                load_lower(jb + 32);
+            else  // the backward sweep starts with its first block, rows [max(n - 32, 0), n)
+                load_upper(n - 32 > 0 ? n - 32 : 0, n - (n - 32 > 0 ? n - 32 : 0));
+        } else {
+            block_gemv<T, TB>(A, n, xs, jb, bw, jb + bw, n, lane, warp - 1, NWS - 1);
+        }
         __syncthreads();
     }
     // backward: U x = y
@@ -635,10 +655,6 @@ __global__ void __launch_bounds__(kGetrsThreads) getrs_kernel(const T* A, int n,
         const int jb = je - 32 > 0 ? je - 32 : 0, bw = je - jb;
         if (warp == 0) {
             TB xv = lane < bw ? xs[jb + lane] : TB(0);
-            T row[32];
-#pragma unroll
-            for (int l = 0; l < 32; ++l)
-                row[l] = (lane < bw && l >= lane && l < bw) ? A[(size_t)(jb + lane) * n + jb + l] : T(1);
 #pragma unroll
             for (int l = 31; l >= 0; --l) {
                 if (l < bw && lane == l) xv = xv / (TB)row[l];
@@ -648,7 +664,11 @@ __global__ void __launch_bounds__(kGetrsThreads) getrs_kernel(const T* A, int n,
             if (lane < bw) xs[jb + lane] = xv;
         }
         __syncthreads();
-        block_gemv<T, TB>(A, n, xs, jb, bw, 0, jb, lane, warp, NWS);
+        if (warp == 0) {
+            if (jb > 0) load_upper(jb - 32 > 0 ? jb - 32 : 0, jb - (jb - 32 > 0 ? jb - 32 : 0));
+        } else {
+            block_gemv<T, TB>(A, n, xs, jb, bw, 0, jb, lane, warp - 1, NWS - 1);
+        }
         __syncthreads();
     }
     for (int i = tid; i < n; i += NT) x[i] = xs[i];
