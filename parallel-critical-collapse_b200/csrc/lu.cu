@@ -423,6 +423,20 @@ __global__ void __launch_bounds__(128) tc_update_kernel(float* A, int n, int k0,
     float* stage = reinterpret_cast<float*>(tc_smem);  // [128][129]: the operands are no longer read
     if (!all_done) {
         if (tid == 0) atomicExch(err, 1);
+        // wait once more, also bounded, for the MMAs still in flight before
+        // the Tensor Memory they write is freed below
+        bool late = done;
+        for (long long it = 0; it < kTcWaitLimit && !late; ++it) {
+            uint32_t ok = 0;
+            asm volatile(
+                "{\n\t.reg .pred P1;\n\t"
+                "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                : "=r"(ok)
+                : "r"(smem_u32(&mbar)), "r"(0)
+                : "memory");
+            late = ok != 0;
+        }
     } else {
         // this warp's 32 lanes = rows 32 warp + lane of the tile, through
         // shared memory so that the update of A22 below is row-coalesced
