@@ -349,13 +349,60 @@ def run_shard(args, world, rank, local):
     eng.close()
 
 
-def cpu_reference(cfg, in0, out0, columns, threads):
+NATIVE_REF = REPO / "oracle" / "_ref" / "native" / "libpcc_ref.so"
+
+
+def host_id():
+    """This host and its CPU model, to tell whether a -march=native build of
+    the reference was made here."""
+    import platform
+
+    model = ""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return f"{platform.node()} | {model}"
+
+
+def build_native_reference():
+    """Rebuilds the compiled reference's library -march=native on this host
+    (as the reference's own build does), from the sources copied into
+    oracle/_ref; returns (path or None, note).  Not timed."""
+    NATIVE_REF.parent.mkdir(parents=True, exist_ok=True)
+    if NATIVE_REF.exists():
+        NATIVE_REF.unlink()
+    env = dict(os.environ, PCC_REF_NATIVE="1")
+    try:
+        r = subprocess.run(["bash", str(REPO / "oracle" / "build_ref.sh")], env=env, capture_output=True,
+                           text=True, timeout=900)
+    except (OSError, subprocess.TimeoutExpired) as e:
+        return None, f"native build failed ({e}); portable x86-64-v3 build used"
+    if r.returncode != 0 or not NATIVE_REF.exists():
+        return None, "native build failed (" + r.stderr.strip()[-200:] + "); portable x86-64-v3 build used"
+    (NATIVE_REF.parent / "host.txt").write_text(host_id())
+    return NATIVE_REF, "-march=native, built on this host before timing"
+
+
+def reference_library():
+    """The compiled reference to time: the -march=native build if it was made
+    on this host, else the portable one."""
+    marker = NATIVE_REF.parent / "host.txt"
+    if NATIVE_REF.exists() and marker.exists() and marker.read_text() == host_id():
+        return NATIVE_REF, "-march=native, built on this host"
+    return REPO / "oracle" / "_ref" / "libpcc_ref.so", "portable x86-64-v3 build"
+
+
+def cpu_reference(cfg, in0, out0, columns, threads, lib=None):
     """Times the reference's own OpenMP Jacobian loop on columns [0, columns):
     (seconds, the columns as rows x columns)."""
     sys.path.insert(0, str(REPO / "tests" / "golden"))
     from ref_lib import RefLib  # compiled reference (oracle/_ref)
 
-    R = RefLib()
+    R = RefLib(lib) if lib else RefLib()
     t = time.perf_counter()
     cols = R.jacobian_columns(cfg, in0, out0, 0, columns, threads)
     return time.perf_counter() - t, cols
@@ -372,13 +419,16 @@ def run_reference(args, world, rank):
     if not (REPO / "oracle" / "_ref" / "libpcc_ref.so").exists():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpcc_ref.so was not built"}))
         return
-    R = RefLib()
+    lib, build_note = build_native_reference()
+    if lib is None:
+        lib = REPO / "oracle" / "_ref" / "libpcc_ref.so"
+    R = RefLib(lib)
     out0 = R.shoot(cfg, in0)
     threads = os.cpu_count() or 1
     cols = min(args.ref_columns or threads, nn)
     for _ in range(args.warmup):
         R.jacobian_columns(cfg, in0, out0, 0, 1, 1)
-    times = [cpu_reference(cfg, in0, out0, cols, threads)[0] for _ in range(args.steps)]
+    times = [cpu_reference(cfg, in0, out0, cols, threads, lib)[0] for _ in range(args.steps)]
     per_build = np.array(times) * nn / cols
     value = 1.0 / float(np.mean(per_build))
     sample = (f"{cols} of {nn} Jacobian columns per step on {threads} threads, extrapolated x{nn / cols:.1f} "
@@ -391,7 +441,7 @@ def run_reference(args, world, rank):
             "impl": "reference",
             "config": workload_config(args, world),
             "cpu_baseline": {"value": value, "unit": "builds/s", "cores": threads, "kind": "reference",
-                             "sample": sample},
+                             "sample": sample, "build": build_note},
             "e2e": {"value": value, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -758,9 +808,11 @@ def run_engine(args, world, rank, local):
         threads = os.cpu_count() or 1
         cols = min(threads, nn)
         if ref_so.exists():
-            t, J_ref = cpu_reference(cfg, in0, out0, cols, threads)
+            lib, build_note = reference_library()
+            t, J_ref = cpu_reference(cfg, in0, out0, cols, threads, lib)
             cpu = {"value": (cols / nn) / t, "unit": "builds/s", "cores": threads, "kind": "reference",
-                   "sample": f"{cols} of {nn} Jacobian columns on {threads} threads ({t:.1f} s), extrapolated"}
+                   "sample": f"{cols} of {nn} Jacobian columns on {threads} threads ({t:.1f} s), extrapolated",
+                   "build": build_note}
             # the timed build's own columns against the reference's on the same input
             J_gpu = h_J.numpy()[:, :cols]
             parity = {"J_rel": float(np.max(np.abs(J_gpu - J_ref)) / np.max(np.abs(J_ref))), "columns": cols,
