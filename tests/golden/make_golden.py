@@ -23,6 +23,8 @@ the full Jacobian is present, the LAPACK Newton update.
 Further cases:
   * c3_seed1024 -- the benchmark's own C3 input (bench.workload(1024, 0.1)):
     its base shoot and 24 reference Jacobian columns (0..15, 508..515);
+  * c1_scheme1, c1_scheme3 -- C1 with SchemeIRK 1 and 3: shoot and four
+    Jacobian columns;
   * c2_newton, c3_newton -- the reference's Newton loop
     (NewtonSolver.cpp:279-366) from a seeded 1e-3 / 1e-4 relative
     perturbation of the near-solution until the mismatch RMS is below 1e-12:
@@ -210,7 +212,7 @@ def newton_case(R, cfg, x0, name, threads, store_jacobian, tol=1e-12, max_iters=
     print(name, "history", hist, flush=True)
 
 
-CASES = ["init_gen", "c1", "c2", "c3", "c3_seed1024", "c2_newton", "c3_newton"]
+CASES = ["init_gen", "c1", "c2", "c3", "c3_seed1024", "c2_newton", "c3_newton", "c1_schemes"]
 
 
 def main():
@@ -252,6 +254,13 @@ def main():
         cfg = config(ref, 512, 3000, 3000)
         z = perturb(packed_input(R, cfg), 1e-3, np.random.default_rng(SEED + 2))
         newton_case(R, cfg, z, "c2_newton", a.threads, store_jacobian=True)
+    if "c1_schemes" in a.cases:
+        # C1 with the one- and three-stage Gauss-Legendre schemes (SchemeIRK 1, 3):
+        # base shoot and the leading column of each field plus Delta
+        for scheme in (1, 3):
+            cfg = config(ref, 128, 1000, 1000)
+            cfg["SchemeIRK"] = scheme
+            case(R, cfg, packed_input(R, cfg), f"c1_scheme{scheme}", [0, 32, 64, 66], a.threads)
     if "c3_newton" in a.cases:
         cfg = config(ref, 1024, 4000, 4000)
         z = perturb(packed_input(R, cfg), 1e-4, np.random.default_rng(SEED + 3))
