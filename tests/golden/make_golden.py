@@ -25,6 +25,10 @@ Further cases:
     its base shoot and 24 reference Jacobian columns (0..15, 508..515);
   * c1_scheme1, c1_scheme3 -- C1 with SchemeIRK 1 and 3: shoot and four
     Jacobian columns;
+  * c256_newton -- the Newton loop at Ntau 256 (2000 + 2000 points), as
+    c2_newton;
+  * c2048 -- Ntau 2048 with the data file's 8000 + 8000 points: boundary
+    data, RHS, IRK steps, the base shoot and Jacobian columns 0..7;
   * c2_newton, c3_newton -- the reference's Newton loop
     (NewtonSolver.cpp:279-366) from a seeded 1e-3 / 1e-4 relative
     perturbation of the near-solution until the mismatch RMS is below 1e-12:
@@ -212,7 +216,8 @@ def newton_case(R, cfg, x0, name, threads, store_jacobian, tol=1e-12, max_iters=
     print(name, "history", hist, flush=True)
 
 
-CASES = ["init_gen", "c1", "c2", "c3", "c3_seed1024", "c2_newton", "c3_newton", "c1_schemes"]
+CASES = ["init_gen", "c1", "c2", "c3", "c3_seed1024", "c2_newton", "c3_newton", "c1_schemes", "c256_newton",
+         "c2048"]
 
 
 def main():
@@ -261,6 +266,23 @@ def main():
             cfg = config(ref, 128, 1000, 1000)
             cfg["SchemeIRK"] = scheme
             case(R, cfg, packed_input(R, cfg), f"c1_scheme{scheme}", [0, 32, 64, 66], a.threads)
+    if "c256_newton" in a.cases:
+        # Ntau 256, 2000 + 2000 points: the Newton loop from a seeded 1e-3 perturbation
+        cfg = config(ref, 256, 2000, 2000)
+        z = perturb(packed_input(R, cfg), 1e-3, np.random.default_rng(SEED + 4))
+        newton_case(R, cfg, z, "c256_newton", a.threads, store_jacobian=True)
+    if "c2048" in a.cases:
+        # Ntau 2048, the data file's 8000 + 8000 points: boundary data, RHS and
+        # IRK steps, the base shoot and Jacobian columns 0..7 (one OpenMP round)
+        cfg = config(ref, 2048, 8000, 8000)
+        case(R, cfg, packed_input(R, cfg), "c2048", None, a.threads)
+        d = dict(np.load(HERE / "ref_c2048.npz"))
+        t = time.time()
+        d["jac_idx"] = np.arange(8)
+        d["jac_cols"] = R.jacobian_columns(cfg, d["in0"], d["out0"], 0, 8, a.threads)
+        d["t_jac_s"] = time.time() - t
+        np.savez_compressed(HERE / "ref_c2048.npz", **d)
+        print("c2048 columns", d["jac_cols"].shape, f"{d['t_jac_s']:.0f} s")
     if "c3_newton" in a.cases:
         cfg = config(ref, 1024, 4000, 4000)
         z = perturb(packed_input(R, cfg), 1e-4, np.random.default_rng(SEED + 3))

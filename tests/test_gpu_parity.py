@@ -22,7 +22,7 @@ from conftest import load_case, rel_err
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["c1_fixture", "c1_perturbed", "c2_fixture", "c3_fixture"]
+CASES = ["c1_fixture", "c1_perturbed", "c2_fixture", "c3_fixture", "c2048"]
 
 
 def _solve(engine, cfg, **over):
@@ -228,6 +228,15 @@ def test_jacobian_columns_c2_c3(engine, name):
     for k, c in enumerate(d["jac_idx"]):
         col = s.jacobian_columns(d["in0"], d["out0"], int(c), int(c) + 1)[:, 0]
         assert np.max(np.abs(col - Jr[:, k])) / scale < 2e-5, c
+
+
+def test_jacobian_columns_c2048(engine):
+    """Columns 0..7 at Ntau 2048 (8000 + 8000 points) in one launch."""
+    d = load_case("c2048")
+    s = _solve(engine, d["cfg"])
+    Jr = d["jac_cols"]
+    J = s.jacobian_columns(d["in0"], d["out0"], 0, Jr.shape[1])
+    assert np.max(np.abs(J - Jr)) / np.max(np.abs(Jr)) < 2e-5
 
 
 @pytest.mark.parametrize("precision", [0, 1])
