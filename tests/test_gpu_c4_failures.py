@@ -17,7 +17,7 @@ import json
 import numpy as np
 import pytest
 
-from conftest import load_case
+from conftest import GOLDEN
 
 pytestmark = pytest.mark.gpu
 
@@ -41,7 +41,7 @@ def _engine_history(engine, cfg, in0):
 
 @pytest.mark.parametrize("i", [6, 14, 15])
 def test_dscan_newton_history_and_end_match_reference(engine, i):
-    d = load_case("c4_failures")
+    d = np.load(GOLDEN / "ref_c4_failures.npz")
     cfg = json.loads(str(d[f"cfg{i}"]))
     ref, ref_end = list(d[f"ref_err{i}"]), str(d[f"ref_end{i}"])
     errs, state = _engine_history(engine, cfg, d[f"in0_{i}"])
