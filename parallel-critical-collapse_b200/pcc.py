@@ -435,9 +435,10 @@ class Solve:
         in0 = _f64(in0)
         out = np.zeros(self.nn)
         st = Stats()
-        self.engine._check(self.lib.pcc_shoot(self.h, _p(in0), _p(out), ctypes.byref(st)))
+        r = self.lib.pcc_shoot(self.h, _p(in0), _p(out), ctypes.byref(st))
         if stats is not None:
-            stats.update(st.as_dict())
+            stats.update(st.as_dict())  # on a failure too: fail_side / fail_grid_index locate it
+        self.engine._check(r)
         return out
 
     def jacobian(self, in0, out0, stats=None):
