@@ -58,3 +58,19 @@ def test_predictor_newton_delta_against_reference(engine):
     i = 2 * ref.size // 3 + 2
     assert abs(xs[0][i] / ref[i] - 1) < 1e-10
     assert np.linalg.norm(xs[0] - ref) / np.linalg.norm(ref) < 1e-4
+
+
+@pytest.mark.parametrize("name", ["c2_newton", "c3_newton"])
+def test_predictor_newton_delta_at_benchmark_sizes(engine, name):
+    """The reference's converged Delta* at Ntau 512 (3000 + 3000 points) and
+    Ntau 1024 (4000 + 4000 points) with the predicted iteration, through the
+    mixed-precision batched Newton loop."""
+    d = load_case(name)
+    s = _solve(engine, d["cfg"], PrecisionNewton=float(d["tol"]), MaxIterNewton=12, IRKPredictor=True)
+    xs, st = engine.newton_solve([s], [d["in0"]], precision=1)
+    s.close()
+    assert st[0]["state"] == "CONVERGED", st
+    ref = d["x_star"]
+    i = 2 * ref.size // 3 + 2
+    assert abs(xs[0][i] / ref[i] - 1) < 1e-10
+    assert np.linalg.norm(xs[0] - ref) / np.linalg.norm(ref) < 1e-6
