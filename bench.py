@@ -446,16 +446,15 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
-def predictor_build(eng, cfg, in0, out0, J_faithful, steps, flush):
-    """C3 Jacobian builds with the optional stage predictor (each step's
-    fixed-point iteration starts from the previous step's collocation
-    polynomial; not in the reference): builds/s and the difference of its
-    Jacobian from the faithful build, relative to max |J|."""
+def variant_build(eng, cfg, in0, out0, J_head, steps, flush, **over):
+    """C3 Jacobian builds of a solve with the SimulationConfig keys over
+    changed: builds/s, RHS evaluations and the difference of its Jacobian
+    from the headline build's J_head, relative to max |J|."""
     import torch
 
     import pcc
 
-    s = eng.solve(pcc.SolveDesc.from_config(dict(cfg, IRKPredictor=True)))
+    s = eng.solve(pcc.SolveDesc.from_config(dict(cfg, **over)))
     nn = s.nn
     d_in0 = torch.tensor(in0, dtype=torch.float64, device="cuda")
     d_out0 = torch.tensor(out0, dtype=torch.float64, device="cuda")
@@ -474,9 +473,33 @@ def predictor_build(eng, cfg, in0, out0, J_faithful, steps, flush):
     s.close()
     return {"builds_per_s": steps / (float(np.sum(ms)) * 1e-3), "ms_per_build": float(np.mean(ms)),
             "rhs_evals_per_build": rhs / steps,
-            "J_diff_vs_faithful_rel_max": float(np.max(np.abs(J - J_faithful)) / np.max(np.abs(J_faithful))),
-            "note": "stage iteration started from the previous step's collocation polynomial (not in the "
-                    "reference); same fixed point to PrecisionIRK"}
+            "J_diff_vs_headline_rel_max": float(np.max(np.abs(J - J_head)) / np.max(np.abs(J_head))),
+            "J_identical": bool(np.array_equal(J, J_head))}
+
+
+def predictor_build(eng, cfg, in0, out0, J_head, steps, flush):
+    """C3 Jacobian builds with the optional stage predictor (each step's
+    fixed-point iteration starts from the previous step's collocation
+    polynomial; not in the reference)."""
+    r = variant_build(eng, cfg, in0, out0, J_head, steps, flush, IRKPredictor=True)
+    r["note"] = ("stage iteration started from the previous step's collocation polynomial (not in the "
+                 "reference); same fixed point to PrecisionIRK")
+    return r
+
+
+def both_sides_build(eng, cfg, in0, out0, J_head, steps, flush):
+    """C3 Jacobian builds in the reference's schedule: every column marches
+    both sides (ShootBothSides); the headline build marches only the side a
+    column's free datum feeds and takes the other from the base shoot."""
+    import pcc
+
+    r = variant_build(eng, cfg, in0, out0, J_head, steps, flush, ShootBothSides=True)
+    n = int(cfg["Ntau"])
+    nn = 3 * n // 4
+    r["sweeps_per_build"] = int(len(pcc.sweep_plan(n, 0, nn, shoot_both_sides=True)))
+    r["headline_sweeps_per_build"] = int(len(pcc.sweep_plan(n, 0, nn)))
+    r["note"] = "every column shoots both sides (NewtonSolver.cpp:615-650 schedule); J_identical compares bits"
+    return r
 
 
 def newton_compare(eng, cfg, in0, out0, J):
@@ -596,7 +619,8 @@ def run_dscan(eng, args):
             "ntau": [int(c["Ntau"]) for c in cfgs], "points": [int(c["NLeft"] + c["NRight"]) for c in cfgs],
             "dims_requested": [float(d) for d in dims], "dims": [float(c["Dim"]) for c in cfgs],
             "wall_s": wall, "jacobian_builds_per_s": len(solves) / wall, "ms_batch_march": st.ms_sweep,
-            "rhs_evals": st.rhs_evals, "sweeps": int(st.shoots) * 2,
+            "rhs_evals": st.rhs_evals,
+            "sweeps": int(sum(len(pcc.sweep_plan(int(c["Ntau"]), 0, 3 * int(c["Ntau"]) // 4)) for c in cfgs)),
             "converge": {"tolerance": tol, "max_iterations": args.dscan_iters, "wall_s": wall_conv,
                          "states": [x["state"] for x in states], "iterations": [x["iterations"] for x in states],
                          "err": [x["err"] for x in states],
@@ -794,6 +818,7 @@ def run_engine(args, world, rank, local):
     # them (after the last collective): another rank's seed need not suit them
     extras = rank == 0 and not args.quick
     predictor = predictor_build(eng, cfg, in0, out0, h_J.numpy().copy(), args.steps, flush) if extras else None
+    both_sides = both_sides_build(eng, cfg, in0, out0, h_J.numpy().copy(), args.steps, flush) if extras else None
     newton = newton_compare(eng, cfg, in0, out0, h_J.numpy().copy()) if extras else None
     dscan = run_dscan(eng, args) if extras else None
     serving = None
@@ -826,7 +851,7 @@ def run_engine(args, world, rank, local):
                 "config": workload_config(args, world),
                 "run": {"sweep_ctas": st_e.sweep_ctas, "wall_s": wall, "march_schedule": eng.march_tuning(n, 2)},
                 "clocks": clk, "e2e": e2e, "gpu_launches": 4 * args.steps, "roofline": roofline,
-                "cpu_baseline": cpu, "parity": parity, "predictor": predictor, "newton_step": newton,
+                "cpu_baseline": cpu, "parity": parity, "predictor": predictor, "both_sides": both_sides, "newton_step": newton,
                 "dscan16": dscan, "serving": serving}
         print(json.dumps(line))
     solve.close()

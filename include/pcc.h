@@ -74,6 +74,14 @@ typedef struct {
                           * (ODEStepper.cpp:202-212); 1 = the previous step's collocation
                           * polynomial, extrapolated (not in the reference: the same fixed
                           * point to round-off, fewer iterations) */
+    int shoot_both_sides; /* 0 (default): a Jacobian column marches only the sides that read
+                          * its free datum (U_p modes: the right side; psi_c and f_c modes:
+                          * the left side; Delta: both) and takes the other side's final
+                          * state from the base shoot, which marched the same boundary
+                          * state bit for bit, so J and the statuses are those of full
+                          * shoots; 1: every column marches both sides, as the reference's
+                          * NewtonSolver::assembleJacobian (NewtonSolver.cpp:615-650, a
+                          * full shoot per column at :639) */
 } pcc_solve_desc;
 
 typedef struct {
@@ -112,6 +120,15 @@ const char* pcc_last_error(pcc_ctx* ctx);
 pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve** out);
 pcc_status pcc_solve_destroy(pcc_solve* s);
 pcc_status pcc_solve_grid(pcc_solve* s, double* grid_out /* nl+nr+1 */);
+
+/* The sweeps that a Jacobian or Newton pipeline over columns [c0, c1) (column
+ * Nnewton = 3 Ntau/4 is the base shoot) of a solve with this Ntau marches, as
+ * slots 2 column + side (0 left, 1 right): right sides first, each side in
+ * column order; with shoot_both_sides = 0 only the sides that read each
+ * column's free datum, plus the base shoot's sides that other columns take
+ * (see pcc_solve_desc.shoot_both_sides).  Writes min(count, cap) slots and
+ * returns the count, or -1 for an invalid Ntau or range.  Needs no device. */
+int pcc_sweep_plan(int ntau, int shoot_both_sides, int c0, int c1, int* slots, int cap);
 
 /* NewtonSolver::shoot (NewtonSolver.cpp:403-423): in0 -> out0, host arrays. */
 pcc_status pcc_shoot(pcc_solve* s, const double* in0, double* out0, pcc_stats* stats);

@@ -340,7 +340,8 @@ __global__ void __launch_bounds__(256) prologue_kernel(BoundaryParams P)
         const int item = item_s;
         __syncthreads();
         if (item >= P.n_items) break;
-        const int col = P.c0 + item / 2, side = item & 1;
+        const int slot = P.sweeps ? P.sweeps[item] : item;
+        const int col = P.sweeps ? slot >> 1 : P.c0 + item / 2, side = slot & 1;
         double* z = B.arr(A_Z);
         for (int k = threadIdx.x; k < P.nn; k += blockDim.x) {
             double v = P.in0[k];
@@ -352,7 +353,7 @@ __global__ void __launch_bounds__(256) prologue_kernel(BoundaryParams P)
         __syncthreads();
         if (threadIdx.x == 0) z[2 * P.nn / 3 + 2] = 0.0;
         __syncthreads();
-        double* y = P.yinit + (size_t)item * P.ntau;
+        double* y = P.yinit + (size_t)slot * P.ntau;
         if (side == 0) {
             unpack_field(B, z, P.nn, 1, B.arr(A_PSIC));
             unpack_field(B, z, P.nn, 2, B.arr(A_FC));
@@ -381,8 +382,14 @@ __global__ void __launch_bounds__(256) epilogue_kernel(BoundaryParams P)
         const int item = item_s;
         __syncthreads();
         if (item >= P.n_items) break;
-        const double* yl = P.yfinal + (size_t)(2 * item) * n;
-        const double* yr = P.yfinal + (size_t)(2 * item + 1) * n;
+        int lcol = item, rcol = item;
+        if (P.abs_slots) {
+            const int col = P.c0 + item;
+            lcol = P.reuse && !column_moves_left(col, P.nn) ? P.nn : col;
+            rcol = P.reuse && !column_moves_right(col, P.nn) ? P.nn : col;
+        }
+        const double* yl = P.yfinal + (size_t)(2 * lcol) * n;
+        const double* yr = P.yfinal + (size_t)(2 * rcol + 1) * n;
         // computeMismatch: yR - yL, Delta guard, Re[2] := Re yL[2]
         double2* mm = B.sb;
         for (int k = threadIdx.x; k < h; k += blockDim.x)

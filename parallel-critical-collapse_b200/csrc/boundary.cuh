@@ -175,16 +175,36 @@ __device__ __forceinline__ double2 double_modes_at(const double2* in, int n_in, 
     return in[k - n_in];
 }
 
+// Which sides of the shoot of column col read the perturbed free datum: the
+// left expansion reads the psi_c and f_c blocks z[nn/3, nn) and Delta, the
+// right expansion the U_p block z[0, nn/3) and Delta (Delta sits at
+// z[2 nn/3 + 2]); column nn is the unperturbed base shoot.  A side that does
+// not read the datum starts from the base shoot's boundary state bit for bit,
+// so its final state is the base shoot's.
+__host__ __device__ __forceinline__ bool column_moves_left(int col, int nn) { return col >= nn / 3; }
+__host__ __device__ __forceinline__ bool column_moves_right(int col, int nn)
+{
+    return col < nn / 3 || col == 2 * nn / 3 + 2 || col >= nn;
+}
+
 struct BoundaryParams {
-    int n_items;        // prologue: 2 per column (left, right); epilogue: 1 per column
+    int n_items;        // prologue: sweeps (2 per column, or sweeps[] entries); epilogue: 1 per column
     int ntau, nn;       // Ntau, Nnewton
     int c0;             // first column of this batch (Nnewton = the unperturbed base shoot)
     double dim, xl, xr, eps, prec;
     double dim_m2_cubed;
     const double* __restrict__ in0;   // Nnewton
     const double* __restrict__ out0;  // Nnewton (finite differencing)
-    double* yinit;                    // [item][N]   (prologue output)
-    const double* yfinal;             // [2*col][N]  (epilogue input)
+    // Sweep slots.  Prologue: with sweeps == null item i is column c0 + i/2,
+    // side i & 1, at slot i; else item i is slot sweeps[i] (2 column + side,
+    // absolute).  Epilogue: with abs_slots == 0 column c0 + i reads slots 2i
+    // and 2i + 1; else column col reads slots 2 col (left) and 2 col + 1
+    // (right), or, with reuse set, the base column's slot of each side col
+    // does not move.
+    const int* sweeps;
+    int abs_slots, reuse;
+    double* yinit;                    // [slot][N]   (prologue output)
+    const double* yfinal;             // [slot][N]   (epilogue input)
     double* outc;                     // [col][Nnewton] packed mismatch per column
     int* status;                      // [col] epilogue: 0 or PCC_ERR_DELTA_MISMATCH
     double* scratch;                  // gridDim.x * kBoundaryArrays * N

@@ -47,6 +47,7 @@ struct MarchParams {
     const double* __restrict__ yinit;  // [item][N], interleaved modes
     double* __restrict__ yfinal;       // [item][N]
     const int* __restrict__ item_side; // optional, else side = item & 1
+    const int* __restrict__ item_map;  // optional (mode 0): work index -> item (slot 2 column + side)
     const double* __restrict__ grid;   // nl + nr + 1
     int nl, nr;
     double dim;
@@ -1194,17 +1195,20 @@ __device__ __forceinline__ void march_item(const SC& sc, const Slot<N, S, PAIR>&
 }
 
 // ------------------------------------------------------------------ kernel
-// The item a sweep slot takes for work index w.  A march over (column, side)
-// items (item = 2 column + side, no explicit side map) hands out every
-// right-side sweep first, then the left-side ones: the right side marches
-// into the stiff x -> 1 end and takes more IRK iterations (22,761 against
-// 16,913 per sweep at Ntau 1024, 4000 + 4000 points), so this hands out the
-// longest sweeps first.  The sweeps and their results are the same in any
-// order.  Measured on that build (1536 sweeps, the same 60.9 M RHS
-// evaluations): 1.187 s against 1.246 s in column order.
+// The item a sweep slot takes for work index w, or -1 when the work is done.
+// With an item map the host has ordered the sweeps.  A march over (column,
+// side) items without one (item = 2 column + side, no explicit side map)
+// hands out every right-side sweep first, then the left-side ones: the right
+// side marches into the stiff x -> 1 end and takes more IRK iterations
+// (22,761 against 16,913 per sweep at Ntau 1024, 4000 + 4000 points), so this
+// hands out the longest sweeps first.  The sweeps and their results are the
+// same in any order.  Measured on that build (1536 sweeps, the same 60.9 M
+// RHS evaluations): 1.187 s against 1.246 s in column order.
 __device__ __forceinline__ int march_item_of(int w, const MarchParams& P)
 {
-    if (P.mode != 0 || P.item_side || (P.n_items & 1) || w >= P.n_items) return w;
+    if (w >= P.n_items) return -1;
+    if (P.item_map) return P.item_map[w];
+    if (P.mode != 0 || P.item_side || (P.n_items & 1)) return w;
     const int h = P.n_items >> 1;
     return w < h ? 2 * w + 1 : 2 * (w - h);
 }
@@ -1225,7 +1229,7 @@ __global__ void __launch_bounds__(MarchShape<N, S, PAIR>::NT, MINB) march_kernel
         sl.sy.sync();
         const int item = *sl.item_slot;
         sl.sy.sync();
-        if (item >= P.n_items) break;
+        if (item < 0) break;
 
         const double* yin = P.yinit + (size_t)item * N;
         const double delta = yin[4];

@@ -213,6 +213,90 @@ MarchParams march_params(pcc_solve* s)
     return P;
 }
 
+bool reuses_sides(const pcc_solve* s) { return s->d.shoot_both_sides == 0; }
+
+// The slot whose final state column col takes for side (0 left, 1 right).
+int source_slot(int nn, bool reuse, int col, int side)
+{
+    const bool moves = side ? column_moves_right(col, nn) : column_moves_left(col, nn);
+    return 2 * (reuse && !moves ? nn : col) + side;
+}
+int source_slot(const pcc_solve* s, int col, int side) { return source_slot(s->nn, reuses_sides(s), col, side); }
+
+// The sweep list of columns [c0, c1) of a solve with nn free data (pcc::sweep_list).
+void sweep_list_of(int nn, bool reuse, int c0, int c1, std::vector<int>& out)
+{
+    out.clear();
+    bool base_needed[2] = {false, false};
+    const bool has_base = c0 <= nn && nn < c1;
+    for (int side = 1; side >= 0; --side) {
+        for (int c = c0; c < c1; ++c) {
+            const int src = source_slot(nn, reuse, c, side);
+            if (src == 2 * c + side)
+                out.push_back(src);
+            else
+                base_needed[side] = true;
+        }
+        if (base_needed[side] && !has_base) out.push_back(2 * nn + side);
+    }
+}
+
+// The device copy of the sweep list of columns [c0, c1) and its length; a
+// range other than the three fixed ones is built and uploaded (stream-ordered
+// on st) when it differs from the last one.
+pcc_status device_sweeps(pcc_solve* s, int c0, int c1, cudaStream_t st, const int** list, int* count)
+{
+    const int nn = s->nn;
+    const std::vector<int>* v = nullptr;
+    int k = 3;
+    if (c0 == 0 && c1 == nn + 1) v = &s->sweeps_build, k = 0;
+    else if (c0 == 0 && c1 == nn) v = &s->sweeps_jac, k = 1;
+    else if (c0 == nn && c1 == nn + 1) v = &s->sweeps_base, k = 2;
+    else {
+        if (c0 != s->range_c0 || c1 != s->range_c1) {
+            sweep_list(s, c0, c1, s->sweeps_range);
+            s->range_c0 = s->range_c1 = -1;
+            PCC_CUDA(s->ctx, cudaMemcpyAsync(s->d_sweeps + s->sweep_off[3], s->sweeps_range.data(),
+                                             s->sweeps_range.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+            s->range_c0 = c0;
+            s->range_c1 = c1;
+        }
+        v = &s->sweeps_range;
+    }
+    *list = s->d_sweeps + s->sweep_off[k];
+    *count = (int)v->size();
+    return PCC_OK;
+}
+
+// The first failure among columns [c0, c1) of the last march and epilogue:
+// the first column (in column order) whose left or right final state (left
+// first, the order a shoot marches them) comes from a sweep that did not
+// converge, else the first column with a Delta mismatch.  st and fi are the
+// march's per-slot statuses and failing grid indices, cs the epilogue's
+// statuses of the columns from c0.  Returns the status and sets col, side
+// (-1 for a Delta mismatch) and the grid index.
+pcc_status first_failure(const pcc_solve* s, int c0, int c1, const std::vector<int>& st,
+                         const std::vector<int>& fi, const std::vector<int>& cs, int* col, int* side, int* idx)
+{
+    *col = *side = *idx = -1;
+    for (int c = c0; c < c1; ++c)
+        for (int sd = 0; sd < 2; ++sd) {
+            const int slot = source_slot(s, c, sd);
+            if (st[slot] != 0) {
+                *col = c;
+                *side = sd;
+                *idx = fi[slot];
+                return PCC_ERR_IRK_NO_CONVERGENCE;
+            }
+        }
+    for (int c = c0; c < c1; ++c)
+        if (cs[c - c0] != 0) {
+            *col = c;
+            return PCC_ERR_DELTA_MISMATCH;
+        }
+    return PCC_OK;
+}
+
 BoundaryParams boundary_params(pcc_solve* s, int c0)
 {
     BoundaryParams B{};
@@ -236,17 +320,42 @@ BoundaryParams boundary_params(pcc_solve* s, int c0)
     return B;
 }
 
-// Boundary data of columns [c0, c1) from d_in0 -> d_yinit (and cleared counters).
+// Boundary data of the sweeps of columns [c0, c1) from d_in0 -> d_yinit (and
+// cleared counters and march statuses: a slot the list leaves out keeps
+// status 0).
 pcc_status enqueue_prologue(pcc_solve* s, int c0, int c1, cudaStream_t st)
 {
     pcc_ctx* ctx = s->ctx;
-    const int items = 2 * (c1 - c0);
+    const int* list = nullptr;
+    int items = 0;
+    pcc_status r = device_sweeps(s, c0, c1, st, &list, &items);
+    if (r != PCC_OK) return r;
     PCC_CUDA(ctx, cudaMemsetAsync(s->d_counters_i, 0, 4 * sizeof(int), st));
     PCC_CUDA(ctx, cudaMemsetAsync(s->d_counters, 0, 4 * sizeof(unsigned long long), st));
+    PCC_CUDA(ctx, cudaMemsetAsync(s->d_status, 0, 2 * (s->nn + 1) * sizeof(int), st));
     BoundaryParams B = boundary_params(s, c0);
     B.n_items = items;
+    B.sweeps = list;
     B.work_counter = s->d_counters_i + 0;
     PCC_CUDA(ctx, launch_prologue(B, boundary_ctas(s, items), st));
+    return PCC_OK;
+}
+
+// The single-solve march over the sweeps of columns [c0, c1) (the list the
+// prologue used).
+pcc_status enqueue_march(pcc_solve* s, int c0, int c1, MarchParams& P, cudaStream_t st)
+{
+    const int* list = nullptr;
+    int items = 0;
+    pcc_status r = device_sweeps(s, c0, c1, st, &list, &items);
+    if (r != PCC_OK) return r;
+    P.n_items = items;
+    P.item_map = list;
+    P.mode = 0;
+    P.yinit = s->d_yinit;
+    P.yfinal = s->d_yfinal;
+    P.work_counter = s->d_counters_i + 1;
+    PCC_CUDA(s->ctx, launch_march(s->d.ntau, s->stages, P, 0, st, &s->last_launch));
     return PCC_OK;
 }
 
@@ -257,6 +366,8 @@ pcc_status enqueue_epilogue(pcc_solve* s, int c0, int c1, bool fd, double* d_J, 
     const int ncols = c1 - c0;
     BoundaryParams B = boundary_params(s, c0);
     B.n_items = ncols;
+    B.abs_slots = 1;
+    B.reuse = reuses_sides(s) ? 1 : 0;
     B.work_counter = s->d_counters_i + 2;
     PCC_CUDA(ctx, launch_epilogue(B, boundary_ctas(s, ncols), st));
     if (fd) {
@@ -289,12 +400,8 @@ pcc_status enqueue_columns(pcc_solve* s, int c0, int c1, bool fd, double* d_J)
     if (r != PCC_OK) return r;
     PCC_CUDA(ctx, record_event(s->ev[1], st));
     MarchParams P = march_params(s);
-    P.n_items = 2 * (c1 - c0);
-    P.mode = 0;
-    P.yinit = s->d_yinit;
-    P.yfinal = s->d_yfinal;
-    P.work_counter = s->d_counters_i + 1;
-    PCC_CUDA(ctx, launch_march(s->d.ntau, s->stages, P, 0, st, &s->last_launch));
+    r = enqueue_march(s, c0, c1, P, st);
+    if (r != PCC_OK) return r;
     PCC_CUDA(ctx, record_event(s->ev[2], st));
     r = enqueue_epilogue(s, c0, c1, fd, d_J, st);
     if (r != PCC_OK) return r;
@@ -308,26 +415,15 @@ pcc_status collect(pcc_solve* s, int c0, int c1, pcc_stats* stats)
     pcc_ctx* ctx = s->ctx;
     PCC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     const int ncols = c1 - c0;
-    std::vector<int> st(2 * ncols), fi(2 * ncols), cs(ncols);
+    std::vector<int> st(2 * (s->nn + 1)), fi(2 * (s->nn + 1)), cs(ncols);
     unsigned long long cnt[4] = {0, 0, 0, 0};
     PCC_CUDA(ctx, cudaMemcpy(st.data(), s->d_status, st.size() * sizeof(int), cudaMemcpyDeviceToHost));
     PCC_CUDA(ctx, cudaMemcpy(fi.data(), s->d_fail, fi.size() * sizeof(int), cudaMemcpyDeviceToHost));
     PCC_CUDA(ctx, cudaMemcpy(cs.data(), s->d_cstatus, cs.size() * sizeof(int), cudaMemcpyDeviceToHost));
     PCC_CUDA(ctx, cudaMemcpy(cnt, s->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
-    pcc_status result = PCC_OK;
-    int fcol = -1, fside = 0, fidx = -1;
-    for (int i = 0; i < 2 * ncols && result == PCC_OK; ++i)
-        if (st[i] != 0) {
-            result = PCC_ERR_IRK_NO_CONVERGENCE;
-            fcol = c0 + i / 2;
-            fside = i & 1;
-            fidx = fi[i];
-        }
-    for (int i = 0; i < ncols && result == PCC_OK; ++i)
-        if (cs[i] != 0) {
-            result = PCC_ERR_DELTA_MISMATCH;
-            fcol = c0 + i;
-        }
+    int fcol = -1, fside = -1, fidx = -1;
+    const pcc_status result = first_failure(s, c0, c1, st, fi, cs, &fcol, &fside, &fidx);
+    if (fside < 0) fside = 0;
     if (stats) {
         float ms[3] = {0, 0, 0};
         cudaEventElapsedTime(&ms[0], s->ev[0], s->ev[1]);
@@ -412,13 +508,14 @@ void ensure_march_tuned(pcc_ctx* ctx, int ntau, int stages, const double2* d_tw,
 }
 
 // One persistent launch over the sweeps of columns [0, ncols[i]) of every
-// solve in v, with the context's own tables.
+// solve in v (ncols nn or nn + 1, their sweep lists), with the context's own
+// tables.
 pcc_status enqueue_batch_march(pcc_ctx* ctx, const std::vector<pcc_solve*>& v, const std::vector<int>& ncols,
                                cudaStream_t st)
 {
     std::vector<BatchItem> items;
     for (size_t i = 0; i < v.size(); ++i)
-        for (int k = 0; k < 2 * ncols[i]; ++k) items.push_back({v[i], k});
+        for (int slot : sweeps_from_zero(v[i], ncols[i])) items.push_back({v[i], slot});
     return batch_march_items(ctx, ctx->batch, items, st, 0);
 }
 
@@ -449,22 +546,11 @@ void batch_stats(pcc_ctx* ctx, const std::vector<int>& ncols, pcc_stats* stats)
 void solve_failure(pcc_solve* s, int ncols, int* col, int* side, int* idx)
 {
     *col = *side = *idx = -1;
-    std::vector<int> st(2 * ncols), fi(2 * ncols), cs(ncols);
+    std::vector<int> st(2 * (s->nn + 1)), fi(2 * (s->nn + 1)), cs(ncols);
     if (cudaMemcpy(st.data(), s->d_status, st.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return;
     cudaMemcpy(fi.data(), s->d_fail, fi.size() * sizeof(int), cudaMemcpyDeviceToHost);
     cudaMemcpy(cs.data(), s->d_cstatus, cs.size() * sizeof(int), cudaMemcpyDeviceToHost);
-    for (int i = 0; i < 2 * ncols; ++i)
-        if (st[i] != 0) {
-            *col = i / 2;
-            *side = i & 1;
-            *idx = fi[i];
-            return;
-        }
-    for (int i = 0; i < ncols; ++i)
-        if (cs[i] != 0) {
-            *col = i;
-            return;
-        }
+    first_failure(s, 0, ncols, st, fi, cs, col, side, idx);
 }
 
 // After the march of one Newton iteration (base column nn and columns 0..nn-1):
@@ -508,6 +594,16 @@ void newton_state_from_dev(const NewtonDev& nd, pcc_newton_state* out)
 
 }  // namespace
 
+void pcc::sweep_list(const pcc_solve* s, int c0, int c1, std::vector<int>& out)
+{
+    sweep_list_of(s->nn, reuses_sides(s), c0, c1, out);
+}
+
+const std::vector<int>& pcc::sweeps_from_zero(const pcc_solve* s, int ncols)
+{
+    return ncols > s->nn ? s->sweeps_build : s->sweeps_jac;
+}
+
 // ------------------------------------------------ shared with the serving loop
 namespace pcc {
 
@@ -518,7 +614,7 @@ size_t solve_footprint(const pcc_solve_desc& d, int sms)
     const size_t dbl = sizeof(double), in = sizeof(int);
     return ngrid * dbl + twiddle_count(n) * sizeof(double2) + 2 * nn * dbl + nn * nn * dbl + 2 * (2 * cols * n * dbl) +
            cols * nn * dbl + 2 * (2 * cols * in) + cols * in + 4 * in + 4 * sizeof(unsigned long long) +
-           (size_t)2 * sms * kBoundaryArrays * n * dbl + 2 * cols * in + 4 * cols * dbl + 2 * cols * in +
+           (size_t)2 * sms * kBoundaryArrays * n * dbl + 2 * cols * in + 8 * cols * in + 4 * cols * dbl + 2 * cols * in +
            sizeof(NewtonDev) + 3 * nn * dbl + nn * in + 4 * in + lu_mixed_work_bytes((int)nn) + in;
 }
 
@@ -567,6 +663,7 @@ pcc_status solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, cudaStream_t a
     ALLOC(s->d_counters, 4 * sizeof(unsigned long long));
     ALLOC(s->d_scratch, (size_t)s->scratch_ctas * kBoundaryArrays * n * sizeof(double));
     ALLOC(s->d_item_side, 2 * cols * sizeof(int));
+    ALLOC(s->d_sweeps, 8 * cols * sizeof(int));
     ALLOC(s->d_xs, 4 * cols * sizeof(double));
     ALLOC(s->d_its, 2 * cols * sizeof(int));
     ALLOC(s->d_newton, sizeof(NewtonDev));
@@ -579,11 +676,22 @@ pcc_status solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, cudaStream_t a
     ALLOC(s->d_cancel, sizeof(int));
 #undef ALLOC
     cudaStream_t st = alloc_st ? alloc_st : ctx->stream;
+    sweep_list(s, 0, nn + 1, s->sweeps_build);
+    sweep_list(s, 0, nn, s->sweeps_jac);
+    sweep_list(s, nn, nn + 1, s->sweeps_base);
+    s->sweep_off[0] = 0;
+    s->sweep_off[1] = 2 * cols;
+    s->sweep_off[2] = 4 * cols;
+    s->sweep_off[3] = 4 * cols + 2;
+    const std::vector<int>* lists[3] = {&s->sweeps_build, &s->sweeps_jac, &s->sweeps_base};
     s->tw_host = twiddles(n);
     cudaError_t e = cudaMemcpyAsync(s->d_tw, s->tw_host.data(), s->tw_host.size() * sizeof(double2),
                                     cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->d_grid, s->grid.data(), s->ngrid * sizeof(double), cudaMemcpyHostToDevice, st);
+    for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+        e = cudaMemcpyAsync(s->d_sweeps + s->sweep_off[k], lists[k]->data(), lists[k]->size() * sizeof(int),
+                            cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->d_cancel, 0, sizeof(int), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->d_newton, 0, sizeof(NewtonDev), st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the host tables may go once copied
@@ -601,7 +709,7 @@ void solve_release(pcc_solve* s)
     void* ptrs[] = {s->d_grid, s->d_tw, s->d_in0, s->d_out0, s->d_J, s->d_yinit, s->d_yfinal, s->d_outc,
                     s->d_status, s->d_fail, s->d_cstatus, s->d_counters_i, s->d_counters, s->d_scratch,
                     s->d_item_side, s->d_xs, s->d_its, s->d_newton, s->d_in0old, s->d_rhs, s->d_dx,
-                    s->d_ipiv, s->d_info, s->d_luw, s->d_cancel};
+                    s->d_ipiv, s->d_info, s->d_luw, s->d_cancel, s->d_sweeps};
     for (void* p : ptrs)
         if (p) {
             if (s->alloc_stream)
@@ -808,6 +916,17 @@ pcc_status pcc_solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, pcc_solve*
     return solve_create(ctx, desc, nullptr, true, out);
 }
 
+int pcc_sweep_plan(int ntau, int shoot_both_sides, int c0, int c1, int* slots, int cap)
+{
+    if (ntau < 4 || ntau % 4 != 0) return -1;
+    const int nn = 3 * ntau / 4;
+    if (c0 < 0 || c1 > nn + 1 || c0 >= c1 || cap < 0 || (cap > 0 && !slots)) return -1;
+    std::vector<int> v;
+    sweep_list_of(nn, shoot_both_sides == 0, c0, c1, v);
+    for (int i = 0; i < (int)v.size() && i < cap; ++i) slots[i] = v[i];
+    return (int)v.size();
+}
+
 pcc_status pcc_solve_destroy(pcc_solve* s)
 {
     if (!s) return PCC_ERR_INVALID_ARG;
@@ -904,14 +1023,10 @@ pcc_status pcc_shoot_debug(pcc_solve* s, const double* in0, double* out0, int de
         if (r != PCC_OK) return r;
         PCC_CUDA(ctx, cudaEventRecord(s->ev[1], st));
         MarchParams P = march_params(s);
-        P.n_items = 2;
-        P.mode = 0;
-        P.yinit = s->d_yinit;
-        P.yfinal = s->d_yfinal;
-        P.work_counter = s->d_counters_i + 1;
         P.snap_slot = d_slot;
         P.snap = d_snap;
-        PCC_CUDA(ctx, launch_march(n, s->stages, P, 0, st, &s->last_launch));
+        r = enqueue_march(s, nn, nn + 1, P, st);
+        if (r != PCC_OK) return r;
         PCC_CUDA(ctx, cudaEventRecord(s->ev[2], st));
         r = enqueue_epilogue(s, nn, nn + 1, false, nullptr, st);
         if (r != PCC_OK) return r;
@@ -1568,12 +1683,8 @@ pcc_status pcc_newton_iterate(pcc_ctx* ctx, int count, pcc_solve* const* solves,
         }
         for (pcc_solve* s : single) {
             MarchParams P = march_params(s);
-            P.n_items = 2 * (s->nn + 1);
-            P.mode = 0;
-            P.yinit = s->d_yinit;
-            P.yfinal = s->d_yfinal;
-            P.work_counter = s->d_counters_i + 1;
-            PCC_CUDA(ctx, launch_march(s->d.ntau, s->stages, P, 0, st, &s->last_launch));
+            pcc_status r = enqueue_march(s, 0, s->nn + 1, P, st);
+            if (r != PCC_OK) return r;
         }
         for (int i = 0; i < count; ++i) {
             pcc_solve* s = solves[i];

@@ -66,6 +66,15 @@ struct pcc_solve {
     double* d_scratch = nullptr;
     int scratch_ctas = 0;
     int* d_item_side = nullptr;   // pcc_sweep
+    // Sweep lists (slots 2 column + side, see pcc::sweep_list) of the column
+    // pipelines: the build over columns [0, nn] (Jacobian and base shoot),
+    // the Jacobian over [0, nn) and the base shoot alone, on the host and in
+    // d_sweeps at sweep_off[0..2]; sweep_off[3] holds the list of the last
+    // other column range (range_c0, range_c1).
+    std::vector<int> sweeps_build, sweeps_jac, sweeps_base, sweeps_range;
+    int* d_sweeps = nullptr;      // [8 (nn + 1)]
+    int sweep_off[4] = {0, 0, 0, 0};
+    int range_c0 = -1, range_c1 = -1;
     double* d_xs = nullptr;       // pcc_sweep / test entry points (x_in, x_out)
     int* d_its = nullptr;
     // device-resident Newton iteration (newton.cu)
@@ -103,6 +112,14 @@ struct BatchItem {
     pcc_solve* s;
     int item;  // 2 column + side
 };
+// The sweeps (slots 2 column + side) a pipeline over columns [c0, c1) marches,
+// right sides first, each side in column order.  With side reuse (the
+// default; pcc_solve_desc.shoot_both_sides = 0) a column marches only the
+// sides that read its free datum, and the base shoot's sides are added where
+// a column takes one of them.
+void sweep_list(const pcc_solve* s, int c0, int c1, std::vector<int>& out);
+// The host list of columns [0, ncols) for ncols = nn (Jacobian) or nn + 1 (build).
+const std::vector<int>& sweeps_from_zero(const pcc_solve* s, int ncols);
 // A solve whose buffers come from cudaMallocAsync on alloc_st (nullptr: cudaMalloc)
 // and which is not registered with its context.
 pcc_status solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, cudaStream_t alloc_st, bool registered,

@@ -284,7 +284,7 @@ bool Server::poll_active()
             if (a.phase == 0) {
                 a.phase = 1;
                 a.next_item = 0;
-                a.n_items = 2 * (a.s->nn + 1);
+                a.n_items = (int)a.s->sweeps_build.size();
                 a.outstanding = 0;
             } else if (a.h_nd->state == kNewtonRunning && !abort) {
                 pcc_status r = newton_prologue(a.s, a.st);
@@ -384,7 +384,7 @@ bool Server::start_launches()
             const int take = std::min({limit, a.n_items - a.next_item,
                                        (int)std::ceil((capacity - ctas) * spc)});
             if (take <= 0) return;
-            for (int j = 0; j < take; ++j) items.push_back({a.s, a.next_item + j});
+            for (int j = 0; j < take; ++j) items.push_back({a.s, a.s->sweeps_build[a.next_item + j]});
             a.next_item += take;
             taken[i] += take;
             ctas += (double)take / spc;

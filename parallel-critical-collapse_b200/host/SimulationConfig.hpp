@@ -20,6 +20,7 @@ struct SimulationConfig {
     int MaxIterIRK;
     real_t Delta = 0.0;
     bool IRKPredictor = false;  // extension key "IRKPredictor" (see pcc_solve_desc::irk_predictor)
+    bool ShootBothSides = false;  // extension key "ShootBothSides" (see pcc_solve_desc::shoot_both_sides)
     vec_real fc, psic, Up;
 
     explicit SimulationConfig(json in)
@@ -34,6 +35,7 @@ struct SimulationConfig {
         SlowError = in["SlowError"];
         MaxIterNewton = in["MaxIterNewton"];
         if (in.contains("IRKPredictor") && !in["IRKPredictor"].is_null()) IRKPredictor = in["IRKPredictor"];
+        if (in.contains("ShootBothSides") && !in["ShootBothSides"].is_null()) ShootBothSides = in["ShootBothSides"];
         Verbose = in["Verbose"];
         Debug = in["Debug"];
         Converged = in["Converged"];
@@ -90,6 +92,7 @@ struct SimulationConfig {
         d.slow_error = SlowError;
         d.max_newton = MaxIterNewton;
         d.irk_predictor = IRKPredictor ? 1 : 0;
+        d.shoot_both_sides = ShootBothSides ? 1 : 0;
         return d;
     }
 

@@ -39,7 +39,7 @@ EXPORTS = ["pcc_ctx_create", "pcc_ctx_destroy", "pcc_status_string", "pcc_last_e
            "pcc_jacobian_batch", "pcc_newton_begin", "pcc_newton_iterate", "pcc_newton_result",
            "pcc_newton_solve", "pcc_serve_start", "pcc_submit", "pcc_poll", "pcc_wait", "pcc_serve_stats",
            "pcc_serve_stop", "pcc_resample_fields", "pcc_shoot_debug", "pcc_jacobian_columns_device",
-           "pcc_march_tuning"]
+           "pcc_march_tuning", "pcc_sweep_plan"]
 
 NEWTON_CODES = ["RUNNING", "CONVERGED", "STOPPED", "MAX_ITER", "IRK_FAILED", "DELTA_MISMATCH", "SINGULAR"]
 
@@ -56,7 +56,8 @@ class SolveDesc(ctypes.Structure):
                 ("xm", ctypes.c_double), ("xr", ctypes.c_double), ("eps_newton", ctypes.c_double),
                 ("nl", ctypes.c_int), ("nr", ctypes.c_int), ("prec_irk", ctypes.c_double),
                 ("scheme", ctypes.c_int), ("max_irk", ctypes.c_int), ("prec_newton", ctypes.c_double),
-                ("slow_error", ctypes.c_double), ("max_newton", ctypes.c_int), ("irk_predictor", ctypes.c_int)]
+                ("slow_error", ctypes.c_double), ("max_newton", ctypes.c_int), ("irk_predictor", ctypes.c_int),
+                ("shoot_both_sides", ctypes.c_int)]
 
     @classmethod
     def from_config(cls, cfg):
@@ -65,7 +66,8 @@ class SolveDesc(ctypes.Structure):
                    float(cfg["XRight"]), float(cfg["EpsNewton"]), int(cfg["NLeft"]), int(cfg["NRight"]),
                    float(cfg["PrecisionIRK"]), int(cfg["SchemeIRK"]), int(cfg["MaxIterIRK"]),
                    float(cfg.get("PrecisionNewton", 1e-14)), float(cfg.get("SlowError", 1e-3)),
-                   int(cfg.get("MaxIterNewton", 100)), int(bool(cfg.get("IRKPredictor", False))))
+                   int(cfg.get("MaxIterNewton", 100)), int(bool(cfg.get("IRKPredictor", False))),
+                   int(bool(cfg.get("ShootBothSides", False))))
 
 
 class Stats(ctypes.Structure):
@@ -184,11 +186,24 @@ def load(path=None):
     L.pcc_shoot_debug.argtypes = [vp, _D, _D, ci, ci, _I, _I, _D, ctypes.POINTER(Stats)]
     L.pcc_jacobian_columns_device.argtypes = [vp, vp, vp, ci, ci, vp]
     L.pcc_march_tuning.argtypes = [vp, ci, ci, _I, _D, _D]
+    L.pcc_sweep_plan.argtypes = [ci, ci, ci, ci, _I, ci]
     for name in EXPORTS:
         if name not in ("pcc_status_string", "pcc_last_error"):
             getattr(L, name).restype = ci
     _lib = L
     return L
+
+
+def sweep_plan(ntau, c0, c1, shoot_both_sides=False):
+    """The sweep slots (2 column + side) a pipeline over columns [c0, c1)
+    marches (pcc_sweep_plan; needs no device)."""
+    L = load()
+    n = L.pcc_sweep_plan(int(ntau), int(bool(shoot_both_sides)), int(c0), int(c1), None, 0)
+    if n < 0:
+        raise PccError(PCC_ERR_INVALID_ARG, "pcc_sweep_plan: invalid Ntau or column range")
+    out = np.zeros(n, dtype=np.int32)
+    L.pcc_sweep_plan(int(ntau), int(bool(shoot_both_sides)), int(c0), int(c1), out.ctypes.data_as(_I), n)
+    return out
 
 
 def _p(a):
@@ -445,9 +460,10 @@ class Solve:
         in0, out0 = _f64(in0), _f64(out0)
         J = np.zeros((self.nn, self.nn))
         st = Stats()
-        self.engine._check(self.lib.pcc_jacobian(self.h, _p(in0), _p(out0), _p(J), ctypes.byref(st)))
+        r = self.lib.pcc_jacobian(self.h, _p(in0), _p(out0), _p(J), ctypes.byref(st))
         if stats is not None:
-            stats.update(st.as_dict())
+            stats.update(st.as_dict())  # on a failure too
+        self.engine._check(r)
         return J
 
     def jacobian_columns(self, in0, out0, c0, c1, stats=None):
@@ -456,10 +472,11 @@ class Solve:
         out0 = _f64(out0) if out0 is not None else None
         cols = np.zeros((c1 - c0, self.nn))
         st = Stats()
-        self.engine._check(self.lib.pcc_jacobian_columns(self.h, _p(in0), _p(out0) if out0 is not None else None,
-                                                         c0, c1, _p(cols), ctypes.byref(st)))
+        r = self.lib.pcc_jacobian_columns(self.h, _p(in0), _p(out0) if out0 is not None else None, c0, c1,
+                                          _p(cols), ctypes.byref(st))
         if stats is not None:
-            stats.update(st.as_dict())
+            stats.update(st.as_dict())  # on a failure too
+        self.engine._check(r)
         return cols.T.copy()
 
     def jacobian_device(self, d_in0, d_out0, d_J):

@@ -11,7 +11,7 @@ from conftest import PKG, REPO
 
 def declared():
     src = (REPO / "include" / "pcc.h").read_text()
-    return sorted(set(re.findall(r"^(?:pcc_status|const char\*)\s+(pcc_[a-z0-9_]+)\(", src, re.M)))
+    return sorted(set(re.findall(r"^(?:pcc_status|const char\*|int)\s+(pcc_[a-z0-9_]+)\(", src, re.M)))
 
 
 def test_library_exports_every_declared_symbol():
