@@ -735,7 +735,7 @@ def run_engine(args, world, rank, local):
     torch.cuda.set_device(local)
     eng = pcc.Engine(local)
     cfg, in0 = workload(rank_seed(args.seed, rank), args.amp)
-    solve = eng.solve(pcc.SolveDesc.from_config(cfg))
+    solve = eng.solve(pcc.SolveDesc.from_config(dict(cfg, ShootBothSides=args.both_sides)))
     nn, n = solve.nn, solve.ntau
     out0 = solve.shoot(in0)  # base shoot (the Newton step's, outside the build)
 
@@ -849,7 +849,9 @@ def run_engine(args, world, rank, local):
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded free data)",
                 "config": workload_config(args, world),
-                "run": {"sweep_ctas": st_e.sweep_ctas, "wall_s": wall, "march_schedule": eng.march_tuning(n, 2)},
+                "run": {"sweep_ctas": st_e.sweep_ctas, "wall_s": wall, "march_schedule": eng.march_tuning(n, 2),
+                        "sweeps_per_build": int(len(pcc.sweep_plan(n, 0, nn, shoot_both_sides=args.both_sides))),
+                        "side_reuse": not args.both_sides},
                 "clocks": clk, "e2e": e2e, "gpu_launches": 4 * args.steps, "roofline": roofline,
                 "cpu_baseline": cpu, "parity": parity, "predictor": predictor, "both_sides": both_sides, "newton_step": newton,
                 "dscan16": dscan, "serving": serving}
@@ -882,6 +884,10 @@ def main():
                          "the Jacobian's column count times a full build)")
     ap.add_argument("--columns", type=int, default=0,
                     help="profiling aid: build only the first C columns (not a benchmark line)")
+    ap.add_argument("--both-sides", action="store_true",
+                    help="every Jacobian column marches both sides (ShootBothSides, the reference's schedule) "
+                         "instead of only the side its free datum feeds; with --columns 148 a profiling case of "
+                         "exactly 296 sweeps (one wave)")
     ap.add_argument("--lu", type=int, default=0,
                     help="profiling aid: pcc_lu_solve, FP64 then mixed, on a seeded n x n system of condition "
                          "number 1e6 (prints the refine reports, not a benchmark line)")
