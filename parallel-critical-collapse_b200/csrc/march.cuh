@@ -48,6 +48,7 @@ struct MarchParams {
     double* __restrict__ yfinal;       // [item][N]
     const int* __restrict__ item_side; // optional, else side = item & 1
     const int* __restrict__ item_map;  // optional (mode 0): work index -> item (slot 2 column + side)
+    int* sched;  // optional (with item_map): kMarchSchedWords zeroed words, see march_claim_ends
     const double* __restrict__ grid;   // nl + nr + 1
     int nl, nr;
     double dim;
@@ -1213,6 +1214,31 @@ __device__ __forceinline__ int march_item_of(int w, const MarchParams& P)
     return w < h ? 2 * w + 1 : 2 * (w - h);
 }
 
+// Two-ended claiming over a longest-first item map (MarchParams::sched):
+// word 0 counts claims, word 1 the items taken from the front, word 2 those
+// taken from the back, words 3.. count the sweep slots that started on each
+// SM (%smid).  A slot of even rank on its SM takes the longest remaining
+// sweep, one of odd rank the shortest, so the two sweeps sharing an SM are
+// a long and a short one.  Claims stop after n_items in total, so the front
+// and back ranges never overlap and every item runs once; %smid only steers
+// the choice (a slot whose SM id is out of range counts as rank 0).
+constexpr int kMarchSchedSms = 512;
+constexpr int kMarchSchedWords = 3 + kMarchSchedSms;
+
+__device__ __forceinline__ unsigned sm_id()
+{
+    unsigned id;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(id));
+    return id;
+}
+
+__device__ __forceinline__ int march_claim_ends(const MarchParams& P, bool front)
+{
+    if (atomicAdd(P.sched, 1) >= P.n_items) return -1;
+    const int w = front ? atomicAdd(P.sched + 1, 1) : P.n_items - 1 - atomicAdd(P.sched + 2, 1);
+    return P.item_map[w];
+}
+
 template <int N, int S, int MINB, int PAIR>
 __global__ void __launch_bounds__(MarchShape<N, S, PAIR>::NT, MINB) march_kernel(MarchParams P)
 {
@@ -1223,9 +1249,20 @@ __global__ void __launch_bounds__(MarchShape<N, S, PAIR>::NT, MINB) march_kernel
     if (sl.lt == 0) *sl.zero = 0;
     const ParamScalars sc{P};
     unsigned long long n_its = 0, n_steps = 0;
+    bool front = true;
+    if (P.sched) {
+        if (sl.lt == 0) {
+            const unsigned id = sm_id();
+            *sl.item_slot = id < (unsigned)kMarchSchedSms ? atomicAdd(P.sched + 3 + id, 1) : 0;
+        }
+        sl.sy.sync();
+        front = (*sl.item_slot & 1) == 0;
+        sl.sy.sync();
+    }
 
     for (;;) {
-        if (sl.lt == 0) *sl.item_slot = march_item_of(atomicAdd(P.work_counter, 1), P);
+        if (sl.lt == 0)
+            *sl.item_slot = P.sched ? march_claim_ends(P, front) : march_item_of(atomicAdd(P.work_counter, 1), P);
         sl.sy.sync();
         const int item = *sl.item_slot;
         sl.sy.sync();
@@ -1272,8 +1309,9 @@ __global__ void __launch_bounds__(MarchShape<N, S, PAIR>::NT, MINB) march_kernel
 // Sweeps of several solves (uneven Ntau, grid sizes and dimensions) in one
 // persistent launch.  Items are grouped into Ntau classes, largest first; a
 // CTA works through the classes in that order, and inside a class every sweep
-// slot pulls its own next (solve, item) from the class counter, so sweeps of
-// different solves share a CTA.  All classes use the same 128-thread CTA and
+// slot pulls its own next (solve, item) from the class's longest-first list,
+// from the front or the back by the slot's rank on its SM (as
+// march_claim_ends), so sweeps of different solves share a CTA.  All classes use the same 128-thread CTA and
 // the same stage count (the Gauss-Legendre tableau is a kernel parameter).
 struct BatchSolve {
     const double* grid;
@@ -1296,7 +1334,9 @@ struct BatchParams {
     int n_classes;
     int cls_ntau[kBatchMaxClasses];
     int cls_begin[kBatchMaxClasses + 1];
-    int* cls_counter;   // [kBatchMaxClasses]
+    int* cls_counter;   // [3 kBatchMaxClasses]: per class the claims and the items taken from the front and the back
+    int* sm_rank;       // [kBatchMaxClasses][kMarchSchedSms]: sweep slots started per class and SM
+                        // (null: every slot claims from the front, in list order)
     double a[3][3], b[3], c[3];
     double lq[3][3];               // as MarchParams::lq
     unsigned long long* counters;  // [0] RHS evaluations [1] IRK iterations [2] steps
@@ -1314,7 +1354,16 @@ struct SweepScalars {
     double dim, dm2c, prec;
     int nl, nr, max_its, side;
     int predictor;
+    int front;  // claims from the front of the class's list (else from the back)
 };
+
+// As march_claim_ends, over class c (n items) of a batch launch.
+__device__ __forceinline__ int batch_claim(const BatchParams& B, int c, int n, int front)
+{
+    int* ctr = B.cls_counter + 3 * c;
+    if (atomicAdd(ctr, 1) >= n) return -1;
+    return front ? atomicAdd(ctr + 1, 1) : n - 1 - atomicAdd(ctr + 2, 1);
+}
 
 struct SmemScalars {
     const SweepScalars* p;
@@ -1366,16 +1415,22 @@ __device__ __forceinline__ void batch_class(const BatchParams& B, int c, double2
     const SmemScalars sc{sp, B};
     const int n = B.cls_begin[c + 1] - B.cls_begin[c];
     unsigned long long c_its = 0, c_steps = 0;  // this slot's sweeps in this class
+    // two-ended claiming over the class's longest-first items, as march_claim_ends
+    if (sl.lt == 0) {
+        const unsigned id = sm_id();
+        const int rank =
+            B.sm_rank && id < (unsigned)kMarchSchedSms ? atomicAdd(B.sm_rank + c * kMarchSchedSms + id, 1) : 0;
+        sp->front = (rank & 1) == 0;
+    }
     for (;;) {
         if (sl.lt == 0) {
-            int i = atomicAdd(&B.cls_counter[c], 1);
-            while (i < n) {
+            int i;
+            for (;;) {
+                i = batch_claim(B, c, n, sp->front);
+                if (i < 0) break;
                 const int2 it = B.items[B.cls_begin[c] + i];
                 const BatchSolve& so = B.solves[it.x];
-                if (so.cancel && *(const volatile int*)so.cancel) {  // the solve no longer needs this sweep
-                    i = atomicAdd(&B.cls_counter[c], 1);
-                    continue;
-                }
+                if (so.cancel && *(const volatile int*)so.cancel) continue;  // the solve no longer needs this sweep
                 sp->grid = so.grid;
                 sp->twN = so.twN;
                 sp->yin = so.yinit + (size_t)it.y * N;
@@ -1396,7 +1451,7 @@ __device__ __forceinline__ void batch_class(const BatchParams& B, int c, double2
         }
         sl.sy.sync();
         const int item = *sl.item_slot;
-        if (item >= n) break;
+        if (item < 0) break;
         const double* yin = sp->yin;
         const double k0 = 2.0 * kPi / yin[4];
         load_state<N, S>(sl, yin);

@@ -355,6 +355,13 @@ pcc_status enqueue_march(pcc_solve* s, int c0, int c1, MarchParams& P, cudaStrea
     P.yinit = s->d_yinit;
     P.yfinal = s->d_yfinal;
     P.work_counter = s->d_counters_i + 1;
+    // two-ended claiming (march_claim_ends) unless PCC_MARCH_ENDS=0; read per
+    // launch, so that a process can compare the two orders
+    const char* ends = std::getenv("PCC_MARCH_ENDS");
+    if (!(ends && std::string(ends) == "0")) {
+        PCC_CUDA(s->ctx, cudaMemsetAsync(s->d_sched, 0, kMarchSchedWords * sizeof(int), st));
+        P.sched = s->d_sched;
+    }
     PCC_CUDA(s->ctx, launch_march(s->d.ntau, s->stages, P, 0, st, &s->last_launch));
     return PCC_OK;
 }
@@ -614,7 +621,7 @@ size_t solve_footprint(const pcc_solve_desc& d, int sms)
     const size_t dbl = sizeof(double), in = sizeof(int);
     return ngrid * dbl + twiddle_count(n) * sizeof(double2) + 2 * nn * dbl + nn * nn * dbl + 2 * (2 * cols * n * dbl) +
            cols * nn * dbl + 2 * (2 * cols * in) + cols * in + 4 * in + 4 * sizeof(unsigned long long) +
-           (size_t)2 * sms * kBoundaryArrays * n * dbl + 2 * cols * in + 8 * cols * in + 4 * cols * dbl + 2 * cols * in +
+           (size_t)2 * sms * kBoundaryArrays * n * dbl + 2 * cols * in + 8 * cols * in + kMarchSchedWords * in + 4 * cols * dbl + 2 * cols * in +
            sizeof(NewtonDev) + 3 * nn * dbl + nn * in + 4 * in + lu_mixed_work_bytes((int)nn) + in;
 }
 
@@ -664,6 +671,7 @@ pcc_status solve_create(pcc_ctx* ctx, const pcc_solve_desc* desc, cudaStream_t a
     ALLOC(s->d_scratch, (size_t)s->scratch_ctas * kBoundaryArrays * n * sizeof(double));
     ALLOC(s->d_item_side, 2 * cols * sizeof(int));
     ALLOC(s->d_sweeps, 8 * cols * sizeof(int));
+    ALLOC(s->d_sched, kMarchSchedWords * sizeof(int));
     ALLOC(s->d_xs, 4 * cols * sizeof(double));
     ALLOC(s->d_its, 2 * cols * sizeof(int));
     ALLOC(s->d_newton, sizeof(NewtonDev));
@@ -709,7 +717,7 @@ void solve_release(pcc_solve* s)
     void* ptrs[] = {s->d_grid, s->d_tw, s->d_in0, s->d_out0, s->d_J, s->d_yinit, s->d_yfinal, s->d_outc,
                     s->d_status, s->d_fail, s->d_cstatus, s->d_counters_i, s->d_counters, s->d_scratch,
                     s->d_item_side, s->d_xs, s->d_its, s->d_newton, s->d_in0old, s->d_rhs, s->d_dx,
-                    s->d_ipiv, s->d_info, s->d_luw, s->d_cancel, s->d_sweeps};
+                    s->d_ipiv, s->d_info, s->d_luw, s->d_cancel, s->d_sweeps, s->d_sched};
     for (void* p : ptrs)
         if (p) {
             if (s->alloc_stream)
@@ -812,7 +820,8 @@ pcc_status batch_march_items(pcc_ctx* ctx, BatchTables& tab, const std::vector<B
     B.cls_begin[B.n_classes] = (int)table.size();
     const size_t o_items = align_up(solves.size() * sizeof(BatchSolve), 16);
     const size_t o_cls = align_up(o_items + table.size() * sizeof(int2), 16);
-    const size_t o_cnt = align_up(o_cls + kBatchMaxClasses * sizeof(int), 16);
+    const size_t o_rank = align_up(o_cls + 3 * kBatchMaxClasses * sizeof(int), 16);
+    const size_t o_cnt = align_up(o_rank + (size_t)kBatchMaxClasses * kMarchSchedSms * sizeof(int), 16);
     const size_t bytes = o_cnt + 4 * sizeof(unsigned long long);
     pcc_status r = batch_tables_reserve(ctx, tab, bytes);
     if (r != PCC_OK) return r;
@@ -844,6 +853,8 @@ pcc_status batch_march_items(pcc_ctx* ctx, BatchTables& tab, const std::vector<B
     B.solves = reinterpret_cast<const BatchSolve*>(d);
     B.items = reinterpret_cast<const int2*>(d + o_items);
     B.cls_counter = reinterpret_cast<int*>(d + o_cls);
+    const char* ends = std::getenv("PCC_MARCH_ENDS");  // 0: claim in list order, as march_claim_ends
+    B.sm_rank = ends && std::string(ends) == "0" ? nullptr : reinterpret_cast<int*>(d + o_rank);
     B.counters = reinterpret_cast<unsigned long long*>(d + o_cnt);
     tab.cnt_off = o_cnt;
     const pcc_solve* s0 = solves[0];

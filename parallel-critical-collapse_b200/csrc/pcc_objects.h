@@ -73,6 +73,7 @@ struct pcc_solve {
     // other column range (range_c0, range_c1).
     std::vector<int> sweeps_build, sweeps_jac, sweeps_base, sweeps_range;
     int* d_sweeps = nullptr;      // [8 (nn + 1)]
+    int* d_sched = nullptr;       // [kMarchSchedWords] two-ended claiming of the single-solve march
     int sweep_off[4] = {0, 0, 0, 0};
     int range_c0 = -1, range_c1 = -1;
     double* d_xs = nullptr;       // pcc_sweep / test entry points (x_in, x_out)

@@ -58,6 +58,23 @@ def test_column_ranges_across_block_edges(engine):
     b.close()
 
 
+def test_claim_order_does_not_change_bits(engine, monkeypatch):
+    """The single-solve march hands its sweeps out from both ends of the
+    longest-first list (by each slot's rank on its SM) unless
+    PCC_MARCH_ENDS=0; which sweep runs where changes no result."""
+    d = load_case("c3_fixture")
+    a, b = _pair(engine, d["cfg"])
+    st_ends, st_plain = {}, {}
+    J_ends = a.jacobian(d["in0"], d["out0"], stats=st_ends)
+    monkeypatch.setenv("PCC_MARCH_ENDS", "0")
+    J_plain = a.jacobian(d["in0"], d["out0"], stats=st_plain)
+    J_both = b.jacobian(d["in0"], d["out0"])
+    assert np.array_equal(J_ends, J_plain) and np.array_equal(J_ends, J_both)
+    assert st_ends["rhs_evals"] == st_plain["rhs_evals"]
+    a.close()
+    b.close()
+
+
 def test_predictor_jacobian_bit_identical(engine):
     d = load_case("c2_fixture")
     a, b = _pair(engine, d["cfg"], IRKPredictor=True)
