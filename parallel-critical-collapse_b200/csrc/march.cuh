@@ -1337,6 +1337,7 @@ struct BatchParams {
     int* cls_counter;   // [3 kBatchMaxClasses]: per class the claims and the items taken from the front and the back
     int* sm_rank;       // [kBatchMaxClasses][kMarchSchedSms]: sweep slots started per class and SM
                         // (null: every slot claims from the front, in list order)
+    int cls_ends[kBatchMaxClasses];  // 1: class c claims from both ends (a few waves deep), 0: list order
     double a[3][3], b[3], c[3];
     double lq[3][3];               // as MarchParams::lq
     unsigned long long* counters;  // [0] RHS evaluations [1] IRK iterations [2] steps
@@ -1418,8 +1419,9 @@ __device__ __forceinline__ void batch_class(const BatchParams& B, int c, double2
     // two-ended claiming over the class's longest-first items, as march_claim_ends
     if (sl.lt == 0) {
         const unsigned id = sm_id();
-        const int rank =
-            B.sm_rank && id < (unsigned)kMarchSchedSms ? atomicAdd(B.sm_rank + c * kMarchSchedSms + id, 1) : 0;
+        const int rank = B.sm_rank && B.cls_ends[c] && id < (unsigned)kMarchSchedSms
+                             ? atomicAdd(B.sm_rank + c * kMarchSchedSms + id, 1)
+                             : 0;
         sp->front = (rank & 1) == 0;
     }
     for (;;) {

@@ -814,6 +814,13 @@ pcc_status batch_march_items(pcc_ctx* ctx, BatchTables& tab, const std::vector<B
         });
         B.cls_ntau[B.n_classes] = n;
         B.cls_begin[B.n_classes] = (int)table.size();
+        // two-ended claiming where the class is at most four waves deep: it
+        // shortens one build's last wave by about 2 %, while four builds in
+        // one launch (ten waves) ran about 1 % slower with it
+        const int spc = n == 128 ? MarchShape<128, 2>::SPC : n == 256 ? MarchShape<256, 2>::SPC
+                        : n == 512 ? MarchShape<512, 2>::SPC : MarchShape<1024, 2>::SPC;
+        const long long slots = (long long)(max_ctas > 0 ? max_ctas : 2 * ctx->sms) * spc;
+        B.cls_ends[B.n_classes] = (long long)cls.size() <= 4 * slots ? 1 : 0;
         for (auto& c : cls) table.push_back(make_int2(sidx[c.second], items[c.second].item));
         B.n_classes += 1;
     }
