@@ -88,7 +88,8 @@ typedef struct {
     long long rhs_evals;      /* RHS evaluations performed on the device */
     long long irk_iterations; /* fixed-point iterations summed over all steps */
     long long irk_steps;      /* grid steps marched */
-    long long shoots;         /* two-sided shoots (Jacobian columns + base) */
+    long long shoots;         /* shoot results delivered (Jacobian columns + base); with side reuse a
+                               * column marches one side (see irk_steps for the sweeps' work) */
     double ms_prologue;       /* boundary data kernel (device time) */
     double ms_sweep;          /* IRK march kernel (device time) */
     double ms_epilogue;       /* mismatch/pack/difference kernels (device time) */
